@@ -1,0 +1,189 @@
+/*
+ * stx.h -- C ABI of the B200 multi-species reacting step (libstx.so).
+ *
+ * The entry points replace the device work that the reference's GPU equation
+ * object (src/multideal/multideal_gpu.F90, type equation_multideal_gpu_object,
+ * :164-211) launches from its type-bound procedures.  Every array argument uses
+ * the reference's own layout, so a Fortran host can pass its allocations as-is:
+ *
+ *   w      (1-ng:nx+ng, 1-ng:ny+ng, 1-ng:nz+ng, nv)      column-major, i fastest
+ *   w_aux  (1-ng:nx+ng, 1-ng:ny+ng, 1-ng:nz+ng, nv_aux)
+ *   fl, fln, fl_sav  (1:nx, 1:ny, 1:nz, nv)
+ *   fluid_mask (1-ng:nx+ng, 1-ng:ny+ng, 1-ng:nz+ng) int32, 0 = fluid (may be NULL)
+ *
+ * with nv = ns+4 and the reference's index map (src/multideal/index_define.h):
+ * species 1..ns, I_U..I_E = ns+1..ns+4; in w_aux the species mass fractions
+ * 1..ns, J_U=ns+1, J_V, J_W, J_H, J_T, J_P, J_C, J_MU, J_DUC, J_DIV, J_R, J_Z,
+ * J_K_COND=ns+13 and rho*D_k at ns+13+k.  Indices in arguments are the
+ * reference's 1-based Fortran indices.
+ *
+ * All field pointers are device pointers; every call is asynchronous on the
+ * caller's stream and allocates nothing on the device, except stx_ctx_create
+ * (tables, scratch) and stx_compute_dt / stx_advance_solution_host, which say
+ * so.  Return value: 0 on success, a negative STX_E_* code otherwise.  Kernels
+ * never trap: iteration caps (Newton, Rosenbrock) set bits in the context's
+ * device status word, read with stx_status().
+ */
+#ifndef STX_H
+#define STX_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STX_ABI_VERSION 1
+
+/* error codes */
+#define STX_OK            0
+#define STX_E_INVALID    -1   /* bad argument (null pointer, range, unsupported option) */
+#define STX_E_CUDA       -2   /* a CUDA runtime call failed */
+#define STX_E_NOMEM      -3   /* device allocation failed (stx_ctx_create only) */
+#define STX_E_UNSUPPORTED -4  /* option outside the supported hot path (e.g. IBM, LES, NR BCs) */
+
+/* status bits accumulated on the device (stx_status) */
+#define STX_ST_NEWTON_CAP     0x1u  /* a Newton T(e) inversion hit its 10-iteration cap */
+#define STX_ST_ROS_STEPS_CAP  0x2u  /* a Rosenbrock cell hit ros_maxsteps */
+#define STX_ST_ROS_TRY_CAP    0x4u  /* a full-Jacobian Rosenbrock step exhausted ros_maxtry */
+#define STX_ST_NONFINITE      0x8u  /* a non-finite value was produced */
+
+/* Property tables: the arrays set_fluid_prop / set_fluid_prop_cantera build
+ * (src/multideal/multideal.F90:2714-3318), in their Fortran layouts. */
+typedef struct stx_tables {
+  int32_t ns, nr;
+  int32_t indx_cp_l, indx_cp_r, nsetcv, num_t_tab;
+  double  t_min_tab, dt_tab, R_univ;
+  const double *mw, *mwinv, *rgas;             /* (ns) */
+  const double *trange;                        /* (ns, nsetcv+1) */
+  const double *cp_coeff, *cv_coeff;           /* (indx_cp_l:indx_cp_r+2, ns, nsetcv), times R_k */
+  const double *visc, *lambda;                 /* (num_t_tab+1, ns) */
+  const double *diffbin;                       /* (num_t_tab+1, ns, ns), at p0 */
+  const int32_t *reac_ty, *is_rev;             /* (nr) */
+  const double *arr_a, *arr_b, *arr_ea;        /* (nr, 2), SI kmol units, Ea in J/kmol */
+  const double *falloff;                       /* (nr, 5) */
+  const double *tb_eff, *r_coeffs, *p_coeffs;  /* (nr, ns) */
+  const double *kc_tab;                        /* (num_t_tab+1, nr), clamped to [tiny, huge] */
+  /* Bilger mixture fraction (multideal.F90:955-1060); n_eoi == 1 gives Z = 0.5 */
+  int32_t n_eoi;
+  const double *aw_eoi, *coeff_eoi;            /* (n_eoi) */
+  const int32_t *nainsp;                       /* (ns, n_eoi) */
+  const double *beta0;                         /* (2) */
+} stx_tables;
+
+/* Grid: local coordinates and metrics (src/field.F90:300-347). */
+typedef struct stx_grid {
+  int32_t nx, ny, nz, ng;
+  const double *x, *y, *z;                     /* (1-ng:n+ng) */
+  const double *dcsidx, *detady, *dzitdz;      /* (n) = 1/dxg */
+  const double *dcsidxs, *detadys, *dzitdzs;   /* (n) squares */
+} stx_grid;
+
+/* Numerics and controls (multideal.ini keys, bc_preproc, runge_kutta_initialize). */
+typedef struct stx_params {
+  int32_t nv_aux;
+  double  p0, rho0, u0, eps_sensor, tol_iter_nr;
+  int32_t ep_order, nkeep, weno_scheme, weno_version, flux_splitting;
+  int32_t sensor_type, visc_order, conservative_viscous;
+  double  sensor_threshold;
+  int32_t bctags[6];                           /* xmin,xmax,ymin,ymax,zmin,zmax; 0 = periodic */
+  int32_t bctags_nr[6];                        /* must be 0 (non-reflecting BCs not on this path) */
+  int32_t force_zero_flux[6];
+  int32_t eul_imin, eul_imax, eul_jmin, eul_jmax, eul_kmin, eul_kmax;
+  int32_t enable_chemistry;                    /* 0 off, 1 explicit source, 2 implicit Rosenbrock */
+  int32_t rosenbrock_version;                  /* 1 full Jacobian, 2 ROK4 Krylov */
+  int32_t operator_splitting;                  /* 1 "simpler", 2 Strang */
+  int32_t ros_maxsteps, ros_maxtry;
+  double  ros_eps;
+  int32_t nrk;                                 /* 3: Wray RK3 */
+  double  rhork[4], gamrk[4];
+  const double *winf;                          /* (nv) free-stream state for bc tag 1, may be NULL */
+} stx_params;
+
+/* Field set of one solve (all device pointers). */
+typedef struct stx_fields {
+  double *w, *w_aux, *fl, *fln, *fl_sav;       /* fl_sav only for operator_splitting == 1 */
+  const int32_t *fluid_mask;                   /* may be NULL: every cell is fluid */
+} stx_fields;
+
+typedef struct stx_ctx stx_ctx;
+
+/* Version of this ABI (STX_ABI_VERSION). */
+int stx_abi_version(void);
+/* Human-readable text of an STX_E_* code. */
+const char *stx_strerror(int code);
+
+/* Create a context on the current CUDA device: validates parameters, copies the
+ * tables and the grid to device memory, allocates scratch.  Replaces the table
+ * upload of multideal_gpu.F90:1361-1424 and the stream set-up of :1468. */
+int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid *grid, stx_ctx **out);
+int stx_ctx_destroy(stx_ctx *ctx);
+
+/* eval_aux_cuf (kernels_gpu.F90:6154-6308): species clip written back into w,
+ * primitives, Newton T(e), c, Bilger Z, Mathur lambda, Wilke mu, Bird rho*D_k,
+ * over the 1-based box [istart,iend]x[jstart,jend]x[kstart,kend]. */
+int stx_eval_aux(stx_ctx *ctx, void *stream, double *w, double *w_aux,
+                 int istart, int iend, int jstart, int jend, int kstart, int kend);
+/* compute_aux (multideal_gpu.F90:361-443): central/ghost selection as in the reference. */
+int stx_compute_aux(stx_ctx *ctx, void *stream, double *w, double *w_aux, int central, int ghost);
+/* eval_aux2_cuf (kernels_gpu.F90:6310-6382): div/3 and the Ducros sensor. */
+int stx_eval_aux2(stx_ctx *ctx, void *stream, double *w_aux);
+/* bcextr_var_cuf (kernels_gpu.F90:5147-5207) on one ghosted scalar field. */
+int stx_bcextr_var(stx_ctx *ctx, void *stream, double *var);
+/* base_gpu%bcswap / bcswap_var (base_gpu.F90:1132-1264) on one GPU: periodic
+ * self-exchange of the ng ghost layers of nvar consecutive ghosted fields. */
+int stx_bcswap(stx_ctx *ctx, void *stream, double *field, int nvar);
+/* update_ghost (multideal_gpu.F90:1165-1238) for bc tags 0,1,2,8; do_swap as in the reference. */
+int stx_update_ghost(stx_ctx *ctx, void *stream, double *w, int do_swap);
+
+/* euler_x/y/z (multideal_gpu.F90:877-1044): hybrid central-KEEP / WENO face
+ * fluxes (kernels_gpu.F90:88-2063) fused with the divergence update
+ * euler_*_update_cuf (:732-793): fl += (fhat_i - fhat_{i-1}) * dxi/dx over
+ * cells [imin,imax].  overwrite != 0 stores instead of accumulating, which
+ * equals the reference's fl = 0 followed by the update. */
+int stx_euler_x(stx_ctx *ctx, void *stream, const double *w_aux, double *fl, int imin, int imax, int overwrite);
+int stx_euler_y(stx_ctx *ctx, void *stream, const double *w_aux, double *fl, int jmin, int jmax, int overwrite);
+int stx_euler_z(stx_ctx *ctx, void *stream, const double *w_aux, double *fl, int kmin, int kmax, int overwrite);
+/* visflx (multideal_gpu.F90:300-359): mode 1 = staggered visflx_x/y/z_cuf with
+ * mixture-averaged diffusion (kernels_gpu.F90:3658-4031) fused with their
+ * divergence; mode 2 = visflx_reduced_cuf (:3539-3656). */
+int stx_visflx(stx_ctx *ctx, void *stream, const double *w_aux, double *fl, int mode);
+
+/* RK bookkeeping (kernels_gpu.F90:11-86, 3297-3355). */
+int stx_init_flux(stx_ctx *ctx, void *stream, double *fl, double *fln, double rhodt);
+int stx_init_flux_simpler(stx_ctx *ctx, void *stream, double *fl, double *fln, const double *fl_sav, double rhodt);
+int stx_sav_flx(stx_ctx *ctx, void *stream, const double *fl, double *fl_sav);
+int stx_update_flux(stx_ctx *ctx, void *stream, const double *fl, double *fln, double gamdt);
+int stx_update_simpler_flux(stx_ctx *ctx, void *stream, const double *fl, double *fln, const double *fl_sav, double gamdt);
+int stx_update_field(stx_ctx *ctx, void *stream, double *w, const double *fln, const int32_t *fluid_mask);
+/* update_flux + update_field fused: fln -= gamdt*(fl - fl_sav?); w += fln (masked). */
+int stx_rk_finish(stx_ctx *ctx, void *stream, double *w, const double *fl, double *fln,
+                  const double *fl_sav, const int32_t *fluid_mask, double gamdt, int simpler);
+
+/* compute_dt_cuf (kernels_gpu.F90:6075-6152): the nine CFL maxima.  Writes
+ * out9 (host memory) after synchronising the stream. */
+int stx_compute_dt(stx_ctx *ctx, void *stream, const double *w_aux, const int32_t *fluid_mask, double out9[9]);
+
+/* Chemistry.  rosenbrock (multideal_gpu.F90:694-753 -> kernels_gpu.F90:8928-9501),
+ * rosenbrock_krylov (:755-837 -> :10360-11205), compute_chemistry (:9503-9674). */
+int stx_rosenbrock(stx_ctx *ctx, void *stream, double *w, double *w_aux,
+                   double dttry, double time_start, double time_end);
+int stx_rosenbrock_krylov(stx_ctx *ctx, void *stream, double *w, const double *w_aux, const double *fl_sav,
+                          double dttry, double time_start, double time_end, int simpler);
+int stx_compute_chemistry(stx_ctx *ctx, void *stream, double *w, double *w_aux, double *fl);
+
+/* Whole steps.  rk_sync (multideal_gpu.F90:536-621) and advance_solution
+ * (:1853-1931) sequenced on the caller's stream; *dt is the step size
+ * (advance_solution halves and restores it for "simpler" splitting exactly
+ * as the reference does).  No host synchronisation inside: capture-safe. */
+int stx_rk_sync(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, int simpler);
+int stx_advance_solution(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, double time);
+
+/* Device status word (OR of STX_ST_* bits since the last reset); synchronises the stream. */
+int stx_status(stx_ctx *ctx, void *stream, uint32_t *bits, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STX_H */
