@@ -1,0 +1,435 @@
+// stx_api.cu -- the extern "C" boundary of libstx.so (include/stx.h): context
+// creation (table upload and repacking), the per-kernel entry points and the
+// rk_sync / advance_solution sequencing on the caller's stream.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "stx_kernels.cuh"
+
+struct stx_ctx {
+  DevCtx d;
+  stx_params par;
+  int periodic[3];
+  int ns, nv;
+  double *winf_d;
+  unsigned int *status_d;         // device status word
+  unsigned int *counter_d;        // work-stealing cell counter of the Rosenbrock kernels
+  unsigned long long *dt_d;       // the nine CFL maxima
+  std::vector<void *> allocs;
+  int device;
+};
+
+namespace {
+
+template <typename T>
+int upload(stx_ctx *c, const T *host, size_t n, const T **out) {
+  void *p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return STX_E_NOMEM;
+  c->allocs.push_back(p);
+  if (host && cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return STX_E_CUDA;
+  if (!host && cudaMemset(p, 0, n * sizeof(T)) != cudaSuccess) return STX_E_CUDA;
+  *out = (const T *)p;
+  return STX_OK;
+}
+
+bool ns_supported(int ns) {
+#define X(N) if (ns == N) return true;
+  STX_FOR_NS(X)
+#undef X
+  return false;
+}
+
+inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+}  // namespace
+
+#define TRY(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_ != STX_OK) return rc_; \
+  } while (0)
+
+extern "C" {
+
+int stx_abi_version(void) { return STX_ABI_VERSION; }
+
+const char *stx_strerror(int code) {
+  switch (code) {
+    case STX_OK: return "ok";
+    case STX_E_INVALID: return "invalid argument";
+    case STX_E_CUDA: return "CUDA runtime error";
+    case STX_E_NOMEM: return "device allocation failed";
+    case STX_E_UNSUPPORTED: return "option outside the supported hot path";
+    default: return "unknown error";
+  }
+}
+
+int stx_ctx_destroy(stx_ctx *c) {
+  if (!c) return STX_E_INVALID;
+  for (void *p : c->allocs) cudaFree(p);
+  delete c;
+  return STX_OK;
+}
+
+int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid *grid, stx_ctx **out) {
+  if (!par || !tab || !grid || !out) return STX_E_INVALID;
+  *out = nullptr;
+  const int ns = tab->ns, nr = tab->nr;
+  if (!ns_supported(ns)) return STX_E_UNSUPPORTED;
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || grid->ng < 1 || grid->ng > 4) return STX_E_INVALID;
+  if (par->nv_aux < 2 * ns + 13) return STX_E_INVALID;
+  if (par->weno_scheme < 1 || par->weno_scheme > 4) return STX_E_INVALID;
+  if (par->ep_order < 2 || par->ep_order > 8 || (par->ep_order & 1)) return STX_E_INVALID;
+  if (par->visc_order < 2 || par->visc_order > 8 || (par->visc_order & 1)) return STX_E_INVALID;
+  if (par->conservative_viscous != 1) return STX_E_UNSUPPORTED;
+  // every stencil (central ep_order/2, viscous visc_order/2, WENO weno_scheme) must fit in the ghost layers
+  if (par->ep_order / 2 > grid->ng || par->visc_order / 2 > grid->ng || par->weno_scheme > grid->ng) return STX_E_INVALID;
+  if (par->nrk < 1 || par->nrk > 4) return STX_E_INVALID;
+  for (int q = 0; q < 6; q++) {
+    int t = par->bctags[q];
+    if (t != 0 && t != 1 && t != 2 && t != 8) return STX_E_UNSUPPORTED;
+    if (par->bctags_nr[q] != 0) return STX_E_UNSUPPORTED;
+  }
+  if (par->eul_imin != 1 || par->eul_imax != grid->nx || par->eul_jmin != 1 || par->eul_jmax != grid->ny ||
+      par->eul_kmin != 1 || par->eul_kmax != grid->nz)
+    return STX_E_UNSUPPORTED;
+  if (tab->nsetcv < 1 || tab->num_t_tab < 1) return STX_E_INVALID;
+  if (par->enable_chemistry > 0 && nr < 1) return STX_E_INVALID;
+  stx_ctx *c = new (std::nothrow) stx_ctx();
+  if (!c) return STX_E_NOMEM;
+  cudaGetDevice(&c->device);
+  c->par = *par;
+  c->ns = ns;
+  c->nv = ns + 4;
+  for (int d = 0; d < 3; d++) c->periodic[d] = par->bctags[2 * d] == 0;
+  DevCtx &d = c->d;
+  DevTab &t = d.t;
+  DevGrid &g = d.g;
+  DevPar &p = d.p;
+  int rc = STX_OK;
+  auto fail = [&](int code) { stx_ctx_destroy(c); return code; };
+  // ---- tables
+  t.ns = ns; t.nr = nr; t.icl = tab->indx_cp_l; t.icr = tab->indx_cp_r; t.nset = tab->nsetcv; t.ntab = tab->num_t_tab;
+  t.ncp = t.icr - t.icl + 3; t.tmin = tab->t_min_tab; t.dtab = tab->dt_tab; t.Ru = tab->R_univ;
+  const size_t ntab1 = (size_t)tab->num_t_tab + 1;
+  if ((rc = upload(c, tab->mw, ns, &t.mw))) return fail(rc);
+  if ((rc = upload(c, tab->mwinv, ns, &t.mwinv))) return fail(rc);
+  if ((rc = upload(c, tab->rgas, ns, &t.rgas))) return fail(rc);
+  if ((rc = upload(c, tab->trange, (size_t)ns * (t.nset + 1), &t.trange))) return fail(rc);
+  if ((rc = upload(c, tab->cp_coeff, (size_t)t.ncp * ns * t.nset, &t.cp))) return fail(rc);
+  if ((rc = upload(c, tab->cv_coeff, (size_t)t.ncp * ns * t.nset, &t.cv))) return fail(rc);
+  {
+    // repack the 1-K tables row-major in temperature so one point reads two contiguous rows
+    std::vector<double> vr(ntab1 * ns), lr(ntab1 * ns), dr(ntab1 * ns * ns);
+    for (size_t it = 0; it < ntab1; it++)
+      for (int k = 0; k < ns; k++) {
+        vr[it * ns + k] = tab->visc[(size_t)k * ntab1 + it];
+        lr[it * ns + k] = tab->lambda[(size_t)k * ntab1 + it];
+        for (int m = 0; m < ns; m++) dr[(it * ns + k) * ns + m] = tab->diffbin[((size_t)m * ns + k) * ntab1 + it];
+      }
+    if ((rc = upload(c, vr.data(), vr.size(), &t.visc_r))) return fail(rc);
+    if ((rc = upload(c, lr.data(), lr.size(), &t.lam_r))) return fail(rc);
+    if ((rc = upload(c, dr.data(), dr.size(), &t.diff_r))) return fail(rc);
+    std::vector<double> wa((size_t)ns * ns), wb((size_t)ns * ns);
+    for (int l = 0; l < ns; l++)
+      for (int m = 0; m < ns; m++) {
+        wa[l * ns + m] = 1.0 / std::sqrt(1.0 + tab->mw[l] * tab->mwinv[m]);
+        wb[l * ns + m] = std::pow(tab->mw[m] * tab->mwinv[l], 0.25);
+      }
+    if ((rc = upload(c, wa.data(), wa.size(), &t.wk_a))) return fail(rc);
+    if ((rc = upload(c, wb.data(), wb.size(), &t.wk_b))) return fail(rc);
+  }
+  if (nr > 0) {
+    if ((rc = upload(c, tab->reac_ty, nr, &t.reac_ty))) return fail(rc);
+    if ((rc = upload(c, tab->is_rev, nr, &t.is_rev))) return fail(rc);
+    if ((rc = upload(c, tab->arr_a, (size_t)nr * 2, &t.arr_a))) return fail(rc);
+    if ((rc = upload(c, tab->arr_b, (size_t)nr * 2, &t.arr_b))) return fail(rc);
+    if ((rc = upload(c, tab->arr_ea, (size_t)nr * 2, &t.arr_ea))) return fail(rc);
+    if ((rc = upload(c, tab->falloff, (size_t)nr * 5, &t.falloff))) return fail(rc);
+    if ((rc = upload(c, tab->tb_eff, (size_t)nr * ns, &t.tb_eff))) return fail(rc);
+    if ((rc = upload(c, tab->r_coeffs, (size_t)nr * ns, &t.r_coeffs))) return fail(rc);
+    if ((rc = upload(c, tab->p_coeffs, (size_t)nr * ns, &t.p_coeffs))) return fail(rc);
+    std::vector<double> kr(ntab1 * nr);
+    for (size_t it = 0; it < ntab1; it++)
+      for (int r = 0; r < nr; r++) kr[it * nr + r] = tab->kc_tab[(size_t)r * ntab1 + it];
+    if ((rc = upload(c, kr.data(), kr.size(), &t.kc_r))) return fail(rc);
+  }
+  t.n_eoi = tab->n_eoi;
+  if (t.n_eoi != 1) {
+    if (t.n_eoi < 1 || !tab->aw_eoi || !tab->coeff_eoi || !tab->beta0 || !tab->nainsp) return fail(STX_E_INVALID);
+    if ((rc = upload(c, tab->aw_eoi, t.n_eoi, &t.aw_eoi))) return fail(rc);
+    if ((rc = upload(c, tab->coeff_eoi, t.n_eoi, &t.coeff_eoi))) return fail(rc);
+    if ((rc = upload(c, tab->beta0, 2, &t.beta0))) return fail(rc);
+    if ((rc = upload(c, tab->nainsp, (size_t)ns * t.n_eoi, &t.nainsp))) return fail(rc);
+  }
+  // ---- grid
+  g.nx = grid->nx; g.ny = grid->ny; g.nz = grid->nz; g.ng = grid->ng;
+  g.nxg = g.nx + 2 * g.ng; g.nyg = g.ny + 2 * g.ng; g.nzg = g.nz + 2 * g.ng;
+  g.npg = (long long)g.nxg * g.nyg * g.nzg;
+  g.npi = (long long)g.nx * g.ny * g.nz;
+  if ((rc = upload(c, grid->x, g.nxg, &g.x))) return fail(rc);
+  if ((rc = upload(c, grid->y, g.nyg, &g.y))) return fail(rc);
+  if ((rc = upload(c, grid->z, g.nzg, &g.z))) return fail(rc);
+  if ((rc = upload(c, grid->dcsidx, g.nx, &g.dcsidx))) return fail(rc);
+  if ((rc = upload(c, grid->detady, g.ny, &g.detady))) return fail(rc);
+  if ((rc = upload(c, grid->dzitdz, g.nz, &g.dzitdz))) return fail(rc);
+  if ((rc = upload(c, grid->dcsidxs, g.nx, &g.dcsidxs))) return fail(rc);
+  if ((rc = upload(c, grid->detadys, g.ny, &g.detadys))) return fail(rc);
+  if ((rc = upload(c, grid->dzitdzs, g.nz, &g.dzitdzs))) return fail(rc);
+  // ---- numerics
+  p.p0 = par->p0; p.rho0 = par->rho0; p.u0 = par->u0; p.eps_sensor = par->eps_sensor; p.tol = par->tol_iter_nr;
+  p.sensor_threshold = par->sensor_threshold; p.ros_eps = par->ros_eps;
+  p.ep_order = par->ep_order; p.nkeep = par->nkeep; p.weno_scheme = par->weno_scheme; p.weno_version = par->weno_version;
+  p.flux_splitting = par->flux_splitting; p.sensor_type = par->sensor_type; p.visc_order = par->visc_order;
+  p.nv_aux = par->nv_aux;
+  for (int q = 0; q < 6; q++) p.fzf[q] = par->force_zero_flux[q];
+  p.ros_maxsteps = par->ros_maxsteps; p.ros_maxtry = par->ros_maxtry;
+  std::memset(p.cd1, 0, sizeof(p.cd1));
+  // coeff_deriv1 (src/grid.F90:135-160), column lmax = order/2
+  p.cd1[1][1] = 0.5;
+  p.cd1[1][2] = 2.0 / 3.0;  p.cd1[2][2] = -1.0 / 12.0;
+  p.cd1[1][3] = 0.75;       p.cd1[2][3] = -0.15;      p.cd1[3][3] = 1.0 / 60.0;
+  p.cd1[1][4] = 4.0 / 5.0;  p.cd1[2][4] = -1.0 / 5.0; p.cd1[3][4] = 4.0 / 105.0; p.cd1[4][4] = -1.0 / 280.0;
+  // ---- device scratch
+  const unsigned int *st = nullptr, *cn = nullptr;
+  const unsigned long long *dtp = nullptr;
+  if ((rc = upload<unsigned int>(c, nullptr, 1, &st))) return fail(rc);
+  if ((rc = upload<unsigned int>(c, nullptr, 1, &cn))) return fail(rc);
+  if ((rc = upload<unsigned long long>(c, nullptr, 9, &dtp))) return fail(rc);
+  c->status_d = (unsigned int *)st;
+  c->counter_d = (unsigned int *)cn;
+  c->dt_d = (unsigned long long *)dtp;
+  p.status = c->status_d;
+  c->winf_d = nullptr;
+  if (par->winf) {
+    const double *wf = nullptr;
+    if ((rc = upload(c, par->winf, (size_t)c->nv, &wf))) return fail(rc);
+    c->winf_d = (double *)wf;
+  }
+  c->par.winf = nullptr;
+  *out = c;
+  return STX_OK;
+}
+
+// ------------------------------------------------------------------ aux
+int stx_eval_aux(stx_ctx *c, void *s, double *w, double *wa, int i0, int i1, int j0, int j1, int k0, int k1) {
+  if (!c || !w || !wa) return STX_E_INVALID;
+  const DevGrid &g = c->d.g;
+  if (i0 < 1 - g.ng || i1 > g.nx + g.ng || j0 < 1 - g.ng || j1 > g.ny + g.ng || k0 < 1 - g.ng || k1 > g.nz + g.ng)
+    return STX_E_INVALID;
+  return launch_eval_aux(c->d, S(s), w, wa, i0, i1, j0, j1, k0, k1);
+}
+
+int stx_eval_aux2(stx_ctx *c, void *s, double *wa) {
+  if (!c || !wa) return STX_E_INVALID;
+  return launch_eval_aux2(c->d, S(s), wa);
+}
+
+int stx_compute_aux(stx_ctx *c, void *s, double *w, double *wa, int central, int ghost) {
+  if (!c || !w || !wa) return STX_E_INVALID;
+  const DevGrid &g = c->d.g;
+  int nx = g.nx, ny = g.ny, nz = g.nz, ng = g.ng;
+  if (central == 1 && ghost == 1) {
+    TRY(stx_eval_aux(c, s, w, wa, 1 - ng, nx + ng, 1 - ng, ny + ng, 1 - ng, nz + ng));
+  } else if (central == 1 && ghost == 0) {
+    TRY(stx_eval_aux(c, s, w, wa, 1, nx, 1, ny, 1, nz));
+  } else if (central == 0 && ghost == 1) {
+    TRY(stx_eval_aux(c, s, w, wa, 1 - ng, 0, 1 - ng, ny + ng, 1 - ng, nz + ng));
+    TRY(stx_eval_aux(c, s, w, wa, nx + 1, nx + ng, 1 - ng, ny + ng, 1 - ng, nz + ng));
+    TRY(stx_eval_aux(c, s, w, wa, 1 - ng, nx + ng, 1 - ng, 0, 1 - ng, nz + ng));
+    TRY(stx_eval_aux(c, s, w, wa, 1 - ng, nx + ng, ny + 1, ny + ng, 1 - ng, nz + ng));
+    TRY(stx_eval_aux(c, s, w, wa, 1 - ng, nx + ng, 1 - ng, ny + ng, 1 - ng, 0));
+    TRY(stx_eval_aux(c, s, w, wa, 1 - ng, nx + ng, 1 - ng, ny + ng, nz + 1, nz + ng));
+  }
+  if (ghost == 1) TRY(stx_eval_aux2(c, s, wa));
+  return STX_OK;
+}
+
+int stx_bcextr_var(stx_ctx *c, void *s, double *v) {
+  if (!c || !v) return STX_E_INVALID;
+  return launch_bcextr_var(c->d, S(s), v);
+}
+
+int stx_bcswap(stx_ctx *c, void *s, double *f, int nvar) {
+  if (!c || !f || nvar < 1) return STX_E_INVALID;
+  return launch_bcswap(c->d, S(s), f, nvar, c->periodic);
+}
+
+int stx_update_ghost(stx_ctx *c, void *s, double *w, int do_swap) {
+  if (!c || !w) return STX_E_INVALID;
+  for (int ilat = 1; ilat <= 6; ilat++) {
+    int tag = c->par.bctags[ilat - 1];
+    if (tag == 1 || tag == 2 || tag == 8) TRY(launch_bc_face(c->d, S(s), w, ilat, tag, c->winf_d));
+  }
+  if (do_swap == 1) TRY(stx_bcswap(c, s, w, c->nv));
+  return STX_OK;
+}
+
+// ------------------------------------------------------------------ fluxes
+int stx_euler_x(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
+  if (!c || !wa || !fl || a < 1 || b > c->d.g.nx) return STX_E_INVALID;
+  return launch_euler(c->d, S(s), 0, wa, fl, a, b, ow);
+}
+int stx_euler_y(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
+  if (!c || !wa || !fl || a < 1 || b > c->d.g.ny) return STX_E_INVALID;
+  return launch_euler(c->d, S(s), 1, wa, fl, a, b, ow);
+}
+int stx_euler_z(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
+  if (!c || !wa || !fl || a < 1 || b > c->d.g.nz) return STX_E_INVALID;
+  return launch_euler(c->d, S(s), 2, wa, fl, a, b, ow);
+}
+
+int stx_visflx(stx_ctx *c, void *s, const double *wa, double *fl, int mode) {
+  if (!c || !wa || !fl) return STX_E_INVALID;
+  const DevGrid &g = c->d.g;
+  if (mode == 1) {
+    if (g.nx > 1) TRY(launch_visflx(c->d, S(s), 0, wa, fl));
+    if (g.ny > 1) TRY(launch_visflx(c->d, S(s), 1, wa, fl));
+    if (g.nz > 1) TRY(launch_visflx(c->d, S(s), 2, wa, fl));
+    return STX_OK;
+  }
+  if (mode == 2) return launch_visflx_reduced(c->d, S(s), wa, fl);
+  return STX_E_UNSUPPORTED;
+}
+
+// ------------------------------------------------------------------ RK
+int stx_init_flux(stx_ctx *c, void *s, double *fl, double *fln, double rhodt) {
+  if (!c || !fl || !fln) return STX_E_INVALID;
+  return launch_init_flux(c->d, S(s), fl, fln, nullptr, rhodt);
+}
+int stx_init_flux_simpler(stx_ctx *c, void *s, double *fl, double *fln, const double *fl_sav, double rhodt) {
+  if (!c || !fl || !fln || !fl_sav) return STX_E_INVALID;
+  return launch_init_flux(c->d, S(s), fl, fln, fl_sav, rhodt);
+}
+int stx_sav_flx(stx_ctx *c, void *s, const double *fl, double *fl_sav) {
+  if (!c || !fl || !fl_sav) return STX_E_INVALID;
+  return launch_copy(c->d, S(s), fl, fl_sav);
+}
+int stx_update_flux(stx_ctx *c, void *s, const double *fl, double *fln, double gamdt) {
+  if (!c || !fl || !fln) return STX_E_INVALID;
+  return launch_update_flux(c->d, S(s), fl, fln, nullptr, gamdt);
+}
+int stx_update_simpler_flux(stx_ctx *c, void *s, const double *fl, double *fln, const double *fl_sav, double gamdt) {
+  if (!c || !fl || !fln || !fl_sav) return STX_E_INVALID;
+  return launch_update_flux(c->d, S(s), fl, fln, fl_sav, gamdt);
+}
+int stx_update_field(stx_ctx *c, void *s, double *w, const double *fln, const int32_t *mask) {
+  if (!c || !w || !fln) return STX_E_INVALID;
+  return launch_update_field(c->d, S(s), w, nullptr, (double *)fln, nullptr, mask, 0.0, 0);
+}
+int stx_rk_finish(stx_ctx *c, void *s, double *w, const double *fl, double *fln, const double *fl_sav,
+                  const int32_t *mask, double gamdt, int simpler) {
+  if (!c || !w || !fl || !fln || (simpler == 1 && !fl_sav)) return STX_E_INVALID;
+  return launch_update_field(c->d, S(s), w, fl, fln, simpler == 1 ? fl_sav : nullptr, mask, gamdt, 1);
+}
+
+int stx_compute_dt(stx_ctx *c, void *s, const double *wa, const int32_t *mask, double out9[9]) {
+  if (!c || !wa || !out9) return STX_E_INVALID;
+  TRY(launch_compute_dt(c->d, S(s), wa, mask, c->dt_d));
+  unsigned long long h[9];
+  STX_CUDA_TRY(cudaMemcpyAsync(h, c->dt_d, sizeof(h), cudaMemcpyDeviceToHost, S(s)));
+  STX_CUDA_TRY(cudaStreamSynchronize(S(s)));
+  for (int q = 0; q < 9; q++) {
+    double v;
+    std::memcpy(&v, &h[q], sizeof(double));
+    out9[q] = v;
+  }
+  return STX_OK;
+}
+
+// ------------------------------------------------------------------ chemistry
+int stx_rosenbrock(stx_ctx *c, void *s, double *w, double *wa, double dttry, double t0, double t1) {
+  if (!c || !w || !wa) return STX_E_INVALID;
+  if (c->d.t.nr < 1) return STX_E_INVALID;
+  return launch_rosenbrock(c->d, S(s), w, wa, dttry, t0, t1, c->counter_d);
+}
+int stx_rosenbrock_krylov(stx_ctx *c, void *s, double *w, const double *wa, const double *fl_sav, double dttry,
+                          double t0, double t1, int simpler) {
+  if (!c || !w || !wa || (simpler == 1 && !fl_sav)) return STX_E_INVALID;
+  if (c->d.t.nr < 1) return STX_E_INVALID;
+  return launch_rok4(c->d, S(s), w, wa, fl_sav, dttry, t0, t1, simpler, c->counter_d);
+}
+int stx_compute_chemistry(stx_ctx *c, void *s, double *w, double *wa, double *fl) {
+  if (!c || !w || !wa || !fl) return STX_E_INVALID;
+  if (c->d.t.nr < 1) return STX_E_INVALID;
+  return launch_chem_explicit(c->d, S(s), w, wa, fl);
+}
+
+// ------------------------------------------------------------------ steps
+static int rhs_pass(stx_ctx *c, void *s, const stx_fields *f) {
+  const int ns = c->ns;
+  const DevGrid &g = c->d.g;
+  double *div = f->w_aux + (size_t)(ns + 9) * g.npg;   // J_DIV (1-based ns+10)
+  double *duc = f->w_aux + (size_t)(ns + 8) * g.npg;   // J_DUC
+  TRY(stx_bcswap(c, s, f->w, c->nv));
+  TRY(stx_compute_aux(c, s, f->w, f->w_aux, 1, 1));
+  TRY(stx_bcextr_var(c, s, div));
+  TRY(stx_bcswap(c, s, duc, 1));
+  TRY(stx_bcswap(c, s, div, 1));
+  TRY(launch_euler(c->d, S(s), 0, f->w_aux, f->fl, c->par.eul_imin, c->par.eul_imax, 0));
+  if (g.ny > 1) TRY(launch_euler(c->d, S(s), 1, f->w_aux, f->fl, c->par.eul_jmin, c->par.eul_jmax, 0));
+  if (g.nz > 1) TRY(launch_euler(c->d, S(s), 2, f->w_aux, f->fl, c->par.eul_kmin, c->par.eul_kmax, 0));
+  TRY(stx_visflx(c, s, f->w_aux, f->fl, 1));
+  TRY(stx_visflx(c, s, f->w_aux, f->fl, 2));
+  if (c->par.enable_chemistry == 1) TRY(stx_compute_chemistry(c, s, f->w, f->w_aux, f->fl));
+  return STX_OK;
+}
+
+int stx_rk_sync(stx_ctx *c, void *s, const stx_fields *f, double dt, int simpler) {
+  if (!c || !f || !f->w || !f->w_aux || !f->fl || !f->fln || (simpler == 1 && !f->fl_sav)) return STX_E_INVALID;
+  for (int istep = 0; istep < c->par.nrk; istep++) {
+    double rhodt = c->par.rhork[istep] * dt;
+    double gamdt = c->par.gamrk[istep] * dt;
+    TRY(launch_init_flux(c->d, S(s), f->fl, f->fln, simpler == 1 ? f->fl_sav : nullptr, rhodt));
+    TRY(rhs_pass(c, s, f));
+    TRY(stx_rk_finish(c, s, f->w, f->fl, f->fln, f->fl_sav, f->fluid_mask, gamdt, simpler));
+    TRY(stx_update_ghost(c, s, f->w, 0));
+  }
+  return STX_OK;
+}
+
+int stx_advance_solution(stx_ctx *c, void *s, const stx_fields *f, double dt, double time) {
+  if (!c || !f || !f->w || !f->w_aux || !f->fl || !f->fln) return STX_E_INVALID;
+  const stx_params &p = c->par;
+  if (p.enable_chemistry == 2) {
+    if (p.operator_splitting == 1) {
+      if (p.rosenbrock_version != 2 || !f->fl_sav) return STX_E_INVALID;
+      double dt_chem = dt;
+      // sav_flx (multideal_gpu.F90:623-692): fl = 0, one right-hand side, fl_sav = fl
+      STX_CUDA_TRY(cudaMemsetAsync(f->fl, 0, sizeof(double) * c->d.g.npi * c->nv, S(s)));
+      TRY(rhs_pass(c, s, f));
+      TRY(stx_update_ghost(c, s, f->w, 0));
+      TRY(stx_sav_flx(c, s, f->fl, f->fl_sav));
+      TRY(stx_compute_aux(c, s, f->w, f->w_aux, 1, 0));
+      TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, f->fl_sav, dt_chem, time, time + dt_chem, 1));
+      TRY(stx_rk_sync(c, s, f, 0.5 * dt, 1));
+    } else {
+      double dt_chem = 0.5 * dt;
+      if (p.rosenbrock_version == 1) TRY(stx_rosenbrock(c, s, f->w, f->w_aux, dt_chem, time, time + dt_chem));
+      else TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, nullptr, dt_chem, time, time + dt_chem, 0));
+      TRY(stx_rk_sync(c, s, f, dt, 0));
+      TRY(stx_compute_aux(c, s, f->w, f->w_aux, 1, 0));
+      if (p.rosenbrock_version == 1) TRY(stx_rosenbrock(c, s, f->w, f->w_aux, dt_chem, time, time + dt_chem));
+      else TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, nullptr, dt_chem, time, time + dt_chem, 0));
+    }
+  } else {
+    TRY(stx_rk_sync(c, s, f, dt, 0));
+  }
+  return STX_OK;
+}
+
+int stx_status(stx_ctx *c, void *s, uint32_t *bits, int reset) {
+  if (!c || !bits) return STX_E_INVALID;
+  unsigned int h = 0;
+  STX_CUDA_TRY(cudaMemcpyAsync(&h, c->status_d, sizeof(h), cudaMemcpyDeviceToHost, S(s)));
+  STX_CUDA_TRY(cudaStreamSynchronize(S(s)));
+  *bits = h;
+  if (reset) STX_CUDA_TRY(cudaMemsetAsync(c->status_d, 0, sizeof(unsigned int), S(s)));
+  return STX_OK;
+}
+
+}  // extern "C"

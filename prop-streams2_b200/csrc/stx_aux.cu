@@ -1,0 +1,470 @@
+// stx_aux.cu -- primitive/transport recovery, Ducros sensor, ghost fills,
+// RK bookkeeping and the CFL reduction (sm_100a).
+//
+// These kernels are HBM-bound stencils or point-wise maps over the reference's
+// SoA fields; each thread owns one point and every field is read and written
+// once with unit-stride (i-fastest) coalesced accesses.
+#include "stx_kernels.cuh"
+
+// ============================================================== eval_aux
+// eval_aux_cuf (kernels_gpu.F90:6154-6308).  Differences in arithmetic order
+// from the reference: the Wilke factor sqrt(mu_m/mu_l) is formed as
+// sqrt(mu_m)*(1/sqrt(mu_l)) and the constant pair factors 1/sqrt(1+W_l/W_m),
+// (W_m/W_l)^0.25 come from a host table; both change results only at rounding
+// level.  The species clip is stored only where it changes w.
+template <int NS>
+__global__ void __launch_bounds__(128) k_eval_aux(DevCtx c, double *__restrict__ w, double *__restrict__ wa,
+                                                  int i0, int j0, int k0, int ni, int nj, int nk) {
+  const DevGrid &g = c.g;
+  const DevTab &t = c.t;
+  long long n = (long long)ni * nj * nk;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= n) return;
+  int i = i0 + (int)(tid % ni);
+  long long r = tid / ni;
+  int j = j0 + (int)(r % nj);
+  int k = k0 + (int)(r / nj);
+  long long p = gidx(g, i, j, k);
+  const int J_U = NS + 1, J_V = NS + 2, J_W = NS + 3, J_H = NS + 4, J_T = NS + 5, J_P = NS + 6, J_C = NS + 7;
+  const int J_MU = NS + 8, J_R = NS + 11, J_Z = NS + 12, J_K = NS + 13;
+  double Y[NS], rw[NS];
+#pragma unroll
+  for (int k2 = 0; k2 < NS; k2++) {
+    double v = FG(w, p, k2 + 1);
+    double vc = v > 0.0 ? v : 0.0;   // max(w, 0); NaN -> 0 as the oracle's max
+    if (__double_as_longlong(vc) != __double_as_longlong(v)) FG(w, p, k2 + 1) = vc;
+    rw[k2] = vc;
+  }
+  double rho = rw[0];
+#pragma unroll
+  for (int k2 = 1; k2 < NS; k2++) rho = rho + rw[k2];
+  double ri = 1.0 / rho;
+#pragma unroll
+  for (int k2 = 0; k2 < NS; k2++) { Y[k2] = rw[k2] * ri; FG(wa, p, k2 + 1) = Y[k2]; }
+  double rhou = FG(w, p, NS + 1), rhov = FG(w, p, NS + 2), rhow = FG(w, p, NS + 3), rhoe = FG(w, p, NS + 4);
+  double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
+  double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+  double ee = rhoe * ri - qq;
+  double tt = temp_from_e<NS>(t, c.p, ee, FG(wa, p, J_T), Y);
+  double rm = ldg(t.rgas) * Y[0];
+#pragma unroll
+  for (int k2 = 1; k2 < NS; k2++) rm = rm + ldg(t.rgas + k2) * Y[k2];
+  double cploc = mix_cp<NS>(t, tt, Y);
+  double gamloc = cploc / (cploc - rm);
+  double pp = rho * tt * rm;
+  double cc = sqrt(gamloc * pp * ri);
+  FG(wa, p, J_R) = rho;
+  FG(wa, p, J_U) = uu;
+  FG(wa, p, J_V) = vv;
+  FG(wa, p, J_W) = ww;
+  FG(wa, p, J_H) = (rhoe + pp) * ri;
+  FG(wa, p, J_T) = tt;
+  FG(wa, p, J_P) = pp;
+  FG(wa, p, J_C) = cc;
+  if (t.n_eoi != 1) {
+    double Beta = 0.0;
+    for (int le = 1; le <= t.n_eoi; le++) {
+      double yatm = 0.0;
+#pragma unroll
+      for (int k2 = 0; k2 < NS; k2++)
+        if (Y[k2] > 1e-14)
+          yatm = yatm + t.nainsp[(long long)(le - 1) * NS + k2] * ldg(t.aw_eoi + le - 1) * Y[k2] * ldg(t.mwinv + k2);
+      Beta = Beta + ldg(t.coeff_eoi + le - 1) * yatm / ldg(t.aw_eoi + le - 1);
+    }
+    FG(wa, p, J_Z) = (Beta - ldg(t.beta0 + 1)) / (ldg(t.beta0) - ldg(t.beta0 + 1));
+  } else {
+    FG(wa, p, J_Z) = 0.5;
+  }
+  int itt;
+  double dtt;
+  table_pos(t, tt, itt, dtt);
+  const double *v0 = t.visc_r + (long long)(itt - 1) * NS, *v1 = v0 + NS;
+  const double *l0 = t.lam_r + (long long)(itt - 1) * NS, *l1 = l0 + NS;
+  double mwmixt = t.Ru / rm;
+  double X[NS];
+#pragma unroll
+  for (int k2 = 0; k2 < NS; k2++) X[k2] = Y[k2] * mwmixt * ldg(t.mwinv + k2);
+  // Mathur
+  double k_cond = 0.0, k_cond2 = 0.0;
+#pragma unroll
+  for (int k2 = 0; k2 < NS; k2++) {
+    double a = ldg(l0 + k2);
+    double klsp = a + (ldg(l1 + k2) - a) * dtt;
+    k_cond = k_cond + X[k2] * klsp;
+    k_cond2 = k_cond2 + X[k2] / klsp;
+  }
+  k_cond = 0.5 * (k_cond + 1.0 / k_cond2);
+  // Wilke
+  double muk[NS], smu[NS];
+#pragma unroll
+  for (int k2 = 0; k2 < NS; k2++) {
+    double a = ldg(v0 + k2);
+    muk[k2] = a + (ldg(v1 + k2) - a) * dtt;
+    smu[k2] = sqrt(muk[k2]);
+  }
+  double mu = 0.0;
+#pragma unroll
+  for (int l = 0; l < NS; l++) {
+    double isl = 1.0 / smu[l];
+    double mu_den = 0.0;
+#pragma unroll
+    for (int m = 0; m < NS; m++) {
+      double t1 = 1.0 + (smu[m] * isl) * ldg(t.wk_b + l * NS + m);
+      double phi_lm = ldg(t.wk_a + l * NS + m) * (t1 * t1);
+      mu_den = mu_den + Y[m] * phi_lm * ldg(t.mwinv + m);
+    }
+    mu = mu + muk[l] * Y[l] * ldg(t.mwinv + l) / mu_den;
+  }
+  mu = sqrt(8.0) * mu;
+  FG(wa, p, J_MU) = mu;
+  FG(wa, p, J_K) = k_cond;
+  // Bird
+  const double *d0 = t.diff_r + (long long)(itt - 1) * NS * NS, *d1 = d0 + NS * NS;
+#pragma unroll
+  for (int l = 0; l < NS; l++) {
+    double diff_den = 0.0;
+#pragma unroll
+    for (int m = 0; m < NS; m++) {
+      if (m != l) {
+        double a = ldg(d0 + l * NS + m);
+        double dij = a + (ldg(d1 + l * NS + m) - a) * dtt;
+        diff_den = diff_den + X[m] / dij;
+      }
+    }
+    FG(wa, p, J_K + 1 + l) = diff_den > 1.0e-15 ? (1.0 - Y[l]) / diff_den * c.p.p0 / pp * rho : 0.0;
+  }
+}
+
+// ============================================================== eval_aux2
+// eval_aux2_cuf (kernels_gpu.F90:6310-6382)
+__global__ void __launch_bounds__(256) k_eval_aux2(DevCtx c, double *__restrict__ wa, int ns) {
+  const DevGrid &g = c.g;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= g.npi) return;
+  int i = 1 + (int)(tid % g.nx);
+  long long r = tid / g.nx;
+  int j = 1 + (int)(r % g.ny);
+  int k = 1 + (int)(r / g.ny);
+  long long p = gidx(g, i, j, k);
+  const int J_U = ns + 1, J_V = ns + 2, J_W = ns + 3, J_DUC = ns + 9, J_DIV = ns + 10;
+  int lmax = c.p.visc_order / 2;
+  long long sx = 1, sy = g.nxg, sz = (long long)g.nxg * g.nyg;
+  double ux = 0, vx = 0, wx = 0, uy = 0, vy = 0, wy = 0, uz = 0, vz = 0, wz = 0;
+  for (int l = 1; l <= lmax; l++) {
+    double ccl = c.p.cd1[l][lmax];
+    ux = ux + ccl * (FG(wa, p + l * sx, J_U) - FG(wa, p - l * sx, J_U));
+    vx = vx + ccl * (FG(wa, p + l * sx, J_V) - FG(wa, p - l * sx, J_V));
+    wx = wx + ccl * (FG(wa, p + l * sx, J_W) - FG(wa, p - l * sx, J_W));
+    uy = uy + ccl * (FG(wa, p + l * sy, J_U) - FG(wa, p - l * sy, J_U));
+    vy = vy + ccl * (FG(wa, p + l * sy, J_V) - FG(wa, p - l * sy, J_V));
+    wy = wy + ccl * (FG(wa, p + l * sy, J_W) - FG(wa, p - l * sy, J_W));
+    uz = uz + ccl * (FG(wa, p + l * sz, J_U) - FG(wa, p - l * sz, J_U));
+    vz = vz + ccl * (FG(wa, p + l * sz, J_V) - FG(wa, p - l * sz, J_V));
+    wz = wz + ccl * (FG(wa, p + l * sz, J_W) - FG(wa, p - l * sz, J_W));
+  }
+  double dx = ldg(g.dcsidx + i - 1), dy = ldg(g.detady + j - 1), dz = ldg(g.dzitdz + k - 1);
+  ux = ux * dx; vx = vx * dx; wx = wx * dx;
+  uy = uy * dy; vy = vy * dy; wy = wy * dy;
+  uz = uz * dz; vz = vz * dz; wz = wz * dz;
+  double div = ux + vy + wz;
+  double div3l = div / 3.0;
+  double ox = wy - vz, oy = uz - wx, oz = vx - uy;
+  double omod2 = ox * ox + oy * oy + oz * oz;
+  double s = -div / sqrt(omod2 + div * div + c.p.eps_sensor);
+  if (c.p.sensor_type == 0) {
+    FG(wa, p, J_DUC) = s * s;
+  } else {
+    double q = s > 0.0 ? s : 0.0;
+    FG(wa, p, J_DUC) = q * q;
+  }
+  FG(wa, p, J_DIV) = div3l;
+}
+
+// ============================================================== ghost fills
+// bcextr_var_cuf (kernels_gpu.F90:5147-5207): all six faces in one launch;
+// sources are interior points, destinations ghosts, so faces are independent.
+__global__ void k_bcextr_var(DevCtx c, double *__restrict__ v) {
+  const DevGrid &g = c.g;
+  long long nxf = (long long)g.ny * g.nz, nyf = (long long)g.nx * g.nz, nzf = (long long)g.nx * g.ny;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int face;
+  long long q;
+  if (tid < 2 * nxf) { face = (int)(tid / nxf); q = tid % nxf; }
+  else if (tid < 2 * nxf + 2 * nyf) { tid -= 2 * nxf; face = 2 + (int)(tid / nyf); q = tid % nyf; }
+  else if (tid < 2 * nxf + 2 * nyf + 2 * nzf) { tid -= 2 * nxf + 2 * nyf; face = 4 + (int)(tid / nzf); q = tid % nzf; }
+  else return;
+  for (int l = 1; l <= g.ng; l++) {
+    if (face == 0) { int j = 1 + (int)(q % g.ny), k = 1 + (int)(q / g.ny); v[gidx(g, 1 - l, j, k)] = v[gidx(g, 1, j, k)]; }
+    if (face == 1) { int j = 1 + (int)(q % g.ny), k = 1 + (int)(q / g.ny); v[gidx(g, g.nx + l, j, k)] = v[gidx(g, g.nx, j, k)]; }
+    if (face == 2) { int i = 1 + (int)(q % g.nx), k = 1 + (int)(q / g.nx); v[gidx(g, i, 1 - l, k)] = v[gidx(g, i, 1, k)]; }
+    if (face == 3) { int i = 1 + (int)(q % g.nx), k = 1 + (int)(q / g.nx); v[gidx(g, i, g.ny + l, k)] = v[gidx(g, i, g.ny, k)]; }
+    if (face == 4) { int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx); v[gidx(g, i, j, 1 - l)] = v[gidx(g, i, j, 1)]; }
+    if (face == 5) { int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx); v[gidx(g, i, j, g.nz + l)] = v[gidx(g, i, j, g.nz)]; }
+  }
+}
+
+// Periodic self-exchange on one GPU, the single-rank case of base_gpu%bcswap
+// (base_gpu.F90:1132-1196, :155-207, :297-383).  One thread per (direction,
+// transverse point, variable) stages the 2*ng source values in registers before
+// writing, which reproduces the reference's pack-then-unpack order even when
+// the extent is smaller than ng; directions read and write disjoint sets.
+#define STX_MAXNG 4
+__global__ void k_bcswap(DevCtx c, double *__restrict__ f, int nvar, int px, int py, int pz) {
+  const DevGrid &g = c.g;
+  long long nxf = px ? (long long)g.ny * g.nz : 0, nyf = py ? (long long)g.nx * g.nz : 0,
+            nzf = pz ? (long long)g.nx * g.ny : 0;
+  long long per = nxf + nyf + nzf;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= per * nvar) return;
+  int m = 1 + (int)(tid / per);
+  long long q = tid % per;
+  int ng = g.ng;
+  double lo[STX_MAXNG], hi[STX_MAXNG];
+  if (q < nxf) {
+    int j = 1 + (int)(q % g.ny), k = 1 + (int)(q / g.ny);
+    for (int i = 1; i <= ng; i++) { lo[i - 1] = FG(f, gidx(g, i, j, k), m); hi[i - 1] = FG(f, gidx(g, g.nx - ng + i, j, k), m); }
+    for (int i = 1; i <= ng; i++) { FG(f, gidx(g, i - ng, j, k), m) = hi[i - 1]; FG(f, gidx(g, g.nx + i, j, k), m) = lo[i - 1]; }
+  } else if (q < nxf + nyf) {
+    q -= nxf;
+    int i = 1 + (int)(q % g.nx), k = 1 + (int)(q / g.nx);
+    for (int j = 1; j <= ng; j++) { lo[j - 1] = FG(f, gidx(g, i, j, k), m); hi[j - 1] = FG(f, gidx(g, i, g.ny - ng + j, k), m); }
+    for (int j = 1; j <= ng; j++) { FG(f, gidx(g, i, j - ng, k), m) = hi[j - 1]; FG(f, gidx(g, i, g.ny + j, k), m) = lo[j - 1]; }
+  } else {
+    q -= nxf + nyf;
+    int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx);
+    for (int k = 1; k <= ng; k++) { lo[k - 1] = FG(f, gidx(g, i, j, k), m); hi[k - 1] = FG(f, gidx(g, i, j, g.nz - ng + k), m); }
+    for (int k = 1; k <= ng; k++) { FG(f, gidx(g, i, j, k - ng), m) = hi[k - 1]; FG(f, gidx(g, i, j, g.nz + k), m) = lo[k - 1]; }
+  }
+}
+
+// update_ghost face kernels: bcfree_cuf (:5073, left side), bcextr_cuf (:5209),
+// bcwall_ad_cuf (:5749).  One launch per face, faces in the reference's order.
+__global__ void k_bc_face(DevCtx c, double *__restrict__ w, int ilat, int tag, int nv, const double *__restrict__ winf) {
+  const DevGrid &g = c.g;
+  int dir = (ilat - 1) / 2, hi = (ilat - 1) % 2;
+  int na = dir == 0 ? g.ny : g.nx, nb = dir == 2 ? g.ny : g.nz;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long per = (long long)na * nb;
+  if (tid >= per * nv) return;
+  int m = 1 + (int)(tid / per);
+  long long q = tid % per;
+  int a = 1 + (int)(q % na), b = 1 + (int)(q / na);
+  int n = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
+  int ns = nv - 4;
+  double sg = (tag == 8 && m >= ns + 1 && m <= ns + 3) ? -1.0 : 1.0;
+  for (int l = 1; l <= g.ng; l++) {
+    int dst = hi ? n + l : 1 - l;
+    int src;
+    if (tag == 2) src = hi ? n : 1;
+    else src = hi ? n + 1 - l : l;   // tag 8
+    int id[3], is[3];
+    if (dir == 0) { id[0] = dst; id[1] = a; id[2] = b; is[0] = src; is[1] = a; is[2] = b; }
+    else if (dir == 1) { id[0] = a; id[1] = dst; id[2] = b; is[0] = a; is[1] = src; is[2] = b; }
+    else { id[0] = a; id[1] = b; id[2] = dst; is[0] = a; is[1] = b; is[2] = src; }
+    long long pd = gidx(g, id[0], id[1], id[2]);
+    if (tag == 1) FG(w, pd, m) = winf[m - 1];
+    else FG(w, pd, m) = sg * FG(w, gidx(g, is[0], is[1], is[2]), m);
+  }
+}
+
+// ============================================================== RK bookkeeping
+// init_flux_cuf / init_flux_simpler_cuf / update_flux_cuf / update_simpler_flux_cuf
+// (kernels_gpu.F90:28-66, 3297-3334); fl is (nx,ny,nz,nv) so these are flat maps.
+__global__ void k_init_flux(double *__restrict__ fl, double *__restrict__ fln, const double *__restrict__ fl_sav,
+                            double rhodt, long long n) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; q < n; q += (long long)gridDim.x * blockDim.x) {
+    double f = fl[q];
+    fln[q] = fl_sav ? -rhodt * (f - fl_sav[q]) : -rhodt * f;
+    fl[q] = 0.0;
+  }
+}
+__global__ void k_update_flux(const double *__restrict__ fl, double *__restrict__ fln, const double *__restrict__ fl_sav,
+                              double gamdt, long long n) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; q < n; q += (long long)gridDim.x * blockDim.x)
+    fln[q] = fl_sav ? fln[q] - gamdt * (fl[q] - fl_sav[q]) : fln[q] - gamdt * fl[q];
+}
+__global__ void k_copy(const double *__restrict__ a, double *__restrict__ b, long long n) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; q < n; q += (long long)gridDim.x * blockDim.x) b[q] = a[q];
+}
+// update_field_cuf (kernels_gpu.F90:3336-3355), optionally fused with
+// update_flux: fln -= gamdt*fl (or gamdt*(fl - fl_sav)); w += fln where fluid.
+__global__ void k_update_field(DevCtx c, double *__restrict__ w, const double *__restrict__ fl, double *__restrict__ fln,
+                               const double *__restrict__ fl_sav, const int32_t *__restrict__ mask, double gamdt,
+                               int fused, int nv) {
+  const DevGrid &g = c.g;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= g.npi) return;
+  int i = 1 + (int)(tid % g.nx);
+  long long r = tid / g.nx;
+  int j = 1 + (int)(r % g.ny);
+  int k = 1 + (int)(r / g.ny);
+  long long p = gidx(g, i, j, k);
+  bool fluid = (mask == nullptr) || (mask[p] == 0);
+  for (int m = 1; m <= nv; m++) {
+    double a;
+    if (fused) {
+      a = fl_sav ? FI(fln, tid, m) - gamdt * (FI(fl, tid, m) - FI(fl_sav, tid, m)) : FI(fln, tid, m) - gamdt * FI(fl, tid, m);
+      FI(fln, tid, m) = a;
+    } else {
+      a = FI(fln, tid, m);
+    }
+    if (fluid) FG(w, p, m) = FG(w, p, m) + a;
+  }
+}
+
+// ============================================================== compute_dt
+// compute_dt_cuf (kernels_gpu.F90:6075-6152): nine maxima, warp shuffles then one
+// atomicMax per block on the bit patterns (non-negative doubles order as integers).
+template <int NS>
+__global__ void __launch_bounds__(256) k_compute_dt(DevCtx c, const double *__restrict__ wa, const int32_t *__restrict__ mask,
+                                                    unsigned long long *__restrict__ out) {
+  const DevGrid &g = c.g;
+  double v[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) v[q] = 0.0;
+  for (long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x; tid < g.npi;
+       tid += (long long)gridDim.x * blockDim.x) {
+    int i = 1 + (int)(tid % g.nx);
+    long long r = tid / g.nx;
+    int j = 1 + (int)(r % g.ny);
+    int k = 1 + (int)(r / g.ny);
+    long long p = gidx(g, i, j, k);
+    if (mask != nullptr && mask[p] != 0) continue;
+    double Y[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) Y[s] = FG(wa, p, s + 1);
+    double rho = FG(wa, p, NS + 11), ri = 1.0 / rho;
+    double uu = FG(wa, p, NS + 1), vv = FG(wa, p, NS + 2), ww = FG(wa, p, NS + 3), tt = FG(wa, p, NS + 5);
+    double mu = FG(wa, p, NS + 8), cc = FG(wa, p, NS + 7), kc = FG(wa, p, NS + 13);
+    double cploc = mix_cp<NS>(c.t, tt, Y);
+    double nu = ri * mu, kr = kc * ri / cploc;
+    double a[9] = {(fabs(uu) + cc) * ldg(g.dcsidx + i - 1), (fabs(vv) + cc) * ldg(g.detady + j - 1),
+                   (fabs(ww) + cc) * ldg(g.dzitdz + k - 1), nu * ldg(g.dcsidxs + i - 1), nu * ldg(g.detadys + j - 1),
+                   nu * ldg(g.dzitdzs + k - 1), kr * ldg(g.dcsidxs + i - 1), kr * ldg(g.detadys + j - 1),
+                   kr * ldg(g.dzitdzs + k - 1)};
+#pragma unroll
+    for (int q = 0; q < 9; q++) v[q] = dmax_(v[q], a[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    for (int o = 16; o > 0; o >>= 1) v[q] = dmax_(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
+  }
+  __shared__ double sm[9][8];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int q = 0; q < 9; q++) sm[q][wid] = v[q];
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    double m = 0.0;
+    for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) m = dmax_(m, sm[threadIdx.x][wv]);
+    atomicMax(out + threadIdx.x, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// ============================================================== launchers
+template <int NS>
+static int eval_aux_t(const DevCtx &c, cudaStream_t s, double *w, double *wa, int i0, int i1, int j0, int j1, int k0, int k1) {
+  int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return STX_OK;
+  long long n = (long long)ni * nj * nk;
+  k_eval_aux<NS><<<grid1d(n, 128), 128, 0, s>>>(c, w, wa, i0, j0, k0, ni, nj, nk);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_eval_aux(const DevCtx &c, cudaStream_t s, double *w, double *wa, int i0, int i1, int j0, int j1, int k0, int k1) {
+  switch (c.t.ns) {
+#define X(N) case N: return eval_aux_t<N>(c, s, w, wa, i0, i1, j0, j1, k0, k1);
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
+}
+
+int launch_eval_aux2(const DevCtx &c, cudaStream_t s, double *wa) {
+  k_eval_aux2<<<grid1d(c.g.npi, 256), 256, 0, s>>>(c, wa, c.t.ns);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_bcextr_var(const DevCtx &c, cudaStream_t s, double *v) {
+  const DevGrid &g = c.g;
+  long long n = 2LL * ((long long)g.ny * g.nz + (long long)g.nx * g.nz + (long long)g.nx * g.ny);
+  k_bcextr_var<<<grid1d(n, 256), 256, 0, s>>>(c, v);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_bcswap(const DevCtx &c, cudaStream_t s, double *f, int nvar, const int *periodic) {
+  const DevGrid &g = c.g;
+  if (g.ng > STX_MAXNG) return STX_E_UNSUPPORTED;
+  long long per = (periodic[0] ? (long long)g.ny * g.nz : 0) + (periodic[1] ? (long long)g.nx * g.nz : 0) +
+                  (periodic[2] ? (long long)g.nx * g.ny : 0);
+  if (per == 0) return STX_OK;
+  k_bcswap<<<grid1d(per * nvar, 256), 256, 0, s>>>(c, f, nvar, periodic[0], periodic[1], periodic[2]);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_bc_face(const DevCtx &c, cudaStream_t s, double *w, int ilat, int tag, const double *winf) {
+  const DevGrid &g = c.g;
+  int dir = (ilat - 1) / 2;
+  int na = dir == 0 ? g.ny : g.nx, nb = dir == 2 ? g.ny : g.nz;
+  int nv = c.t.ns + 4;
+  if (tag == 1 && (ilat != 1 || winf == nullptr)) return STX_OK;   // bcfree_cuf acts on the left side only
+  long long n = (long long)na * nb * nv;
+  k_bc_face<<<grid1d(n, 256), 256, 0, s>>>(c, w, ilat, tag, nv, winf);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt) {
+  long long n = c.g.npi * (c.t.ns + 4);
+  int nb = grid1d(n, 256);
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_init_flux<<<nb, 256, 0, s>>>(fl, fln, fl_sav, rhodt, n);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_update_flux(const DevCtx &c, cudaStream_t s, const double *fl, double *fln, const double *fl_sav, double gamdt) {
+  long long n = c.g.npi * (c.t.ns + 4);
+  int nb = grid1d(n, 256);
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_update_flux<<<nb, 256, 0, s>>>(fl, fln, fl_sav, gamdt, n);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_copy(const DevCtx &c, cudaStream_t s, const double *a, double *b) {
+  long long n = c.g.npi * (c.t.ns + 4);
+  int nb = grid1d(n, 256);
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_copy<<<nb, 256, 0, s>>>(a, b, n);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_update_field(const DevCtx &c, cudaStream_t s, double *w, const double *fl, double *fln, const double *fl_sav,
+                        const int32_t *mask, double gamdt, int fused) {
+  k_update_field<<<grid1d(c.g.npi, 256), 256, 0, s>>>(c, w, fl, fln, fl_sav, mask, gamdt, fused, c.t.ns + 4);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_compute_dt(const DevCtx &c, cudaStream_t s, const double *wa, const int32_t *mask, unsigned long long *out9) {
+  STX_CUDA_TRY(cudaMemsetAsync(out9, 0, 9 * sizeof(unsigned long long), s));
+  int nb = grid1d(c.g.npi, 256);
+  if (nb > 148 * 8) nb = 148 * 8;
+  switch (c.t.ns) {
+#define X(N) case N: k_compute_dt<N><<<nb, 256, 0, s>>>(c, wa, mask, out9); break;
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}

@@ -1,0 +1,209 @@
+// stx_common.cuh -- device-side context, indexing and thermodynamics shared by
+// the sm_100a kernels of libstx.so.
+//
+// Layouts are the reference's (src/multideal/multideal_gpu.F90:1481-1502):
+// ghosted SoA fields w(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,m), i fastest.  The
+// species count is a template parameter so that per-species vectors live in
+// registers; the host dispatches on the runtime value (STX_FOR_NS below).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/stx.h"
+
+#define STX_MMAX 4     // Krylov dimension M_max (index_define.h:27)
+#define STX_NSTAGE 4   // ROK4 stages (index_define.h:4)
+
+// species counts compiled into the library
+#define STX_FOR_NS(X) X(9) X(11) X(13) X(14)
+
+struct DevTab {
+  int ns, nr, icl, icr, nset, ntab, ncp;
+  double tmin, dtab, Ru;
+  const double *mw, *mwinv, *rgas;
+  const double *trange;           // (ns, nset+1)
+  const double *cp, *cv;          // (ncp, ns, nset)
+  const double *visc_r, *lam_r;   // repacked [it][lsp]
+  const double *diff_r;           // repacked [it][lsp][msp] (msp fastest)
+  const int *reac_ty, *is_rev;
+  const double *arr_a, *arr_b, *arr_ea, *falloff;   // (nr,2) / (nr,5)
+  const double *tb_eff, *r_coeffs, *p_coeffs;       // (nr, ns)
+  const double *kc_r;             // repacked [it][lr]
+  const double *wk_a, *wk_b;      // Wilke pair factors [l][m]
+  int n_eoi;
+  const double *aw_eoi, *coeff_eoi, *beta0;
+  const int *nainsp;
+};
+
+struct DevGrid {
+  int nx, ny, nz, ng, nxg, nyg, nzg;
+  long long npg, npi;
+  const double *x, *y, *z;
+  const double *dcsidx, *detady, *dzitdz, *dcsidxs, *detadys, *dzitdzs;
+};
+
+struct DevPar {
+  double p0, rho0, u0, eps_sensor, tol, sensor_threshold, ros_eps;
+  int ep_order, nkeep, weno_scheme, weno_version, flux_splitting, sensor_type, visc_order, nv_aux;
+  int fzf[6];
+  int ros_maxsteps, ros_maxtry;
+  double cd1[5][5];               // coeff_deriv1(l, lmax) -> cd1[l][lmax]
+  unsigned int *status;           // device status word
+};
+
+struct DevCtx {
+  DevTab t;
+  DevGrid g;
+  DevPar p;
+};
+
+// ---------------------------------------------------------------- indexing
+__device__ __forceinline__ long long gidx(const DevGrid &g, int i, int j, int k) {
+  return (long long)(i + g.ng - 1) + (long long)g.nxg * ((long long)(j + g.ng - 1) + (long long)g.nyg * (long long)(k + g.ng - 1));
+}
+__device__ __forceinline__ long long fidx(const DevGrid &g, int i, int j, int k) {
+  return (long long)(i - 1) + (long long)g.nx * ((long long)(j - 1) + (long long)g.ny * (long long)(k - 1));
+}
+// field m (1-based) of a ghosted array
+#define FG(a, p, m) ((a)[(p) + (long long)((m) - 1) * g.npg])
+#define FI(a, q, m) ((a)[(q) + (long long)((m) - 1) * g.npi])
+
+__device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
+
+// Fortran real**integer (the same repeated product as the oracle)
+__device__ __forceinline__ double ipow(double x, int n) {
+  double r = 1.0;
+  int u = n < 0 ? -n : n;
+  for (int q = 0; q < u; q++) r *= x;
+  return n < 0 ? 1.0 / r : r;
+}
+__device__ __forceinline__ double dmax_(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin_(double a, double b) { return a < b ? a : b; }
+
+__device__ __forceinline__ void set_status(const DevPar &p, unsigned bits) {
+  if (p.status) atomicOr(p.status, bits);
+}
+
+// ---------------------------------------------------------------- thermo
+__device__ __forceinline__ double trange_(const DevTab &t, int lsp, int jm) {
+  return ldg(t.trange + (long long)(jm - 1) * t.ns + lsp - 1);
+}
+__device__ __forceinline__ double cpc(const DevTab &t, const double *arr, int l, int lsp, int m) {
+  return ldg(arr + ((long long)(m - 1) * t.ns + lsp - 1) * t.ncp + (l - t.icl));
+}
+
+// Numerical-Recipes locate (kernels_gpu.F90:6397-6415)
+__device__ __forceinline__ int locate_range(const DevTab &t, double T, int lsp) {
+  int jl = 0, ju = t.nset + 2;
+  while (ju - jl > 1) {
+    int jm = (ju + jl) / 2;
+    if (T >= trange_(t, lsp, jm)) jl = jm; else ju = jm;
+  }
+  if (jl < 1) jl = 1;
+  if (jl > t.nset) jl = t.nset;
+  return jl;
+}
+
+// get_cp_dev (kernels_gpu.F90:6384-6432)
+template <int NS>
+__device__ double mix_cp(const DevTab &t, double tt, const double *Y) {
+  int nrange[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) nrange[k] = 1;
+  if (t.nset > 1) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) nrange[k] = locate_range(t, tt, k + 1);
+  }
+  double cploc = 0.0;
+  for (int l = t.icl; l <= t.icr; l++) {
+    double tpow = ipow(tt, l);
+    double cp_l = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) cp_l = cp_l + cpc(t, t.cp, l, k + 1, nrange[k]) * Y[k];
+    cploc = cploc + cp_l * tpow;
+  }
+  return cploc;
+}
+
+// get_mixture_temperature_from_e_dev (kernels_gpu.F90:6532-6622)
+template <int NS>
+__device__ double temp_from_e(const DevTab &t, const DevPar &p, double ee, double T_start, const double *Y) {
+  int nrange[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) nrange[k] = 1;
+  if (t.nset > 1) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) nrange[k] = locate_range(t, T_start, k + 1);
+  }
+  double T_old = T_start, tt = T_start;
+  bool conv = false;
+  for (int iter = 1; iter <= 10; iter++) {
+    if (t.nset > 1) {
+#pragma unroll
+      for (int k = 0; k < NS; k++) {
+        int nl = nrange[k];
+        if (T_old < trange_(t, k + 1, nl)) nrange[k] = nrange[k] - 1;
+        else if (T_old > trange_(t, k + 1, nl + 1)) nrange[k] = nrange[k] + 1;
+        if (nrange[k] < 1) nrange[k] = 1;
+        if (nrange[k] > t.nset) nrange[k] = t.nset;
+      }
+    }
+    double sumb = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) sumb = sumb + cpc(t, t.cv, t.icr + 1, k + 1, nrange[k]) * Y[k];
+    double ebar = ee - sumb;
+    double den = 0.0, num = 0.0;
+    for (int l = t.icl; l <= t.icr; l++) {
+      double T_pow = ipow(T_old, l);
+      double tden = T_pow, tnum;
+      if (l == -1) {
+        tnum = log(T_old);
+      } else {
+        double T_powp = T_old * T_pow;
+        tnum = T_powp / (l + 1.0);
+      }
+      double cv_l = 0.0;
+#pragma unroll
+      for (int k = 0; k < NS; k++) cv_l = cv_l + cpc(t, t.cv, l, k + 1, nrange[k]) * Y[k];
+      num = num + cv_l * tnum;
+      den = den + cv_l * tden;
+    }
+    tt = T_old + (ebar - num) / den;
+    if (fabs(tt - T_old) < p.tol) { conv = true; break; }
+    T_old = tt;
+  }
+  if (!conv) set_status(p, STX_ST_NEWTON_CAP);
+  return tt;
+}
+
+// get_species_h/e_from_temperature_dev (kernels_gpu.F90:7104-7183)
+__device__ __forceinline__ double species_poly_int(const DevTab &t, const double *arr, double tt, int isp) {
+  int nr = 1;
+  if (t.nset > 1) nr = locate_range(t, tt, isp);
+  double hh = cpc(t, arr, t.icr + 1, isp, nr);
+  for (int l = t.icl; l <= t.icr; l++) {
+    if (l == -1) hh = hh + cpc(t, arr, l, isp, nr) * log(tt);
+    else hh = hh + cpc(t, arr, l, isp, nr) / (l + 1.0) * ipow(tt, l + 1);
+  }
+  return hh;
+}
+
+// table row index and fraction (kernels_gpu.F90:6245-6249)
+__device__ __forceinline__ void table_pos(const DevTab &t, double tt, int &itt, double &dtt) {
+  itt = (int)((tt - t.tmin) / t.dtab) + 1;
+  if (itt < 1) itt = 1;
+  if (itt > t.ntab) itt = t.ntab;
+  double tloc = t.tmin + (itt - 1) * t.dtab;
+  dtt = (tt - tloc) / t.dtab;
+}
+
+// ---------------------------------------------------------------- launch helpers
+#define STX_CUDA_TRY(x)                          \
+  do {                                           \
+    cudaError_t e_ = (x);                        \
+    if (e_ != cudaSuccess) return STX_E_CUDA;    \
+  } while (0)
+
+inline int grid1d(long long n, int block) {
+  long long b = (n + block - 1) / block;
+  return (int)(b < 1 ? 1 : b);
+}

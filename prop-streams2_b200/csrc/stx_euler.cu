@@ -1,0 +1,611 @@
+// stx_euler.cu -- hybrid central-KEEP / WENO convective fluxes fused with their
+// divergence (euler_{x,y,z} of src/multideal/multideal_gpu.F90:877-1044 and the
+// kernels of src/multideal/kernels_gpu.F90:88-2063, 2065-3295).
+//
+// B200 design:
+//  * x sweep: one CTA of 128 threads per pencil segment; thread t computes face
+//    f0+t, the faces go through shared memory and threads 1..127 apply
+//    fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- no fhat round trip through HBM.
+//  * y/z sweeps: threads along the contiguous i index (coalesced), each thread
+//    marches a chunk of faces along the sweep keeping the previous face flux
+//    in registers; one redundant face per chunk.
+//  * WENO faces use the structure of the multi-species eigenvectors
+//    (kernels_gpu.F90:2703-2984): the species block of L is identity + rank one,
+//    so every characteristic variable follows from two per-point scalars
+//    (Q = sum_k b1i_k W_k - b2 u.W_mom + b2 W_E and sigma = sum_k W_k): O(ns)
+//    per stencil point instead of O(ns^2).  The back projection keeps the
+//    reference's summation order.  Results equal the reference's dense
+//    products up to rounding.
+#include "stx_kernels.cuh"
+
+// wenorec_1d / wenorec_1d_rusanov (kernels_gpu.F90:2065-2637) for one variable;
+// vp/vm indexed by stencil slot 1..2*ws (slot 0 unused).
+__device__ __forceinline__ double weno_rec(const double *vp, const double *vm, int i, int ord, int version, double bs) {
+  if (ord == 1) return vp[i] + vm[i + 1];
+  if (ord == 2) {
+    double t, bp0, bp1, bm0, bm1;
+    t = vp[i] - vp[i - 1]; bp0 = bs * (t * t);
+    t = vp[i + 1] - vp[i]; bp1 = bs * (t * t);
+    t = vm[i + 2] - vm[i + 1]; bm0 = bs * (t * t);
+    t = vm[i + 1] - vm[i]; bm1 = bs * (t * t);
+    t = 0.000001 + bp0; bp0 = (1.0 / 3.0) / (t * t);
+    t = 0.000001 + bm0; bm0 = (1.0 / 3.0) / (t * t);
+    t = 0.000001 + bp1; bp1 = (2.0 / 3.0) / (t * t);
+    t = 0.000001 + bm1; bm1 = (2.0 / 3.0) / (t * t);
+    double sp = bp0 + bp1, sm = bm0 + bm1;
+    bp0 = bp0 / sp; bp1 = bp1 / sp; bm0 = bm0 / sm; bm1 = bm1 / sm;
+    double vminus = bp0 * (-vp[i - 1] + 3 * vp[i]) + bp1 * (vp[i] + vp[i + 1]);
+    double vplus = bm0 * (-vm[i + 2] + 3 * vm[i + 1]) + bm1 * (vm[i] + vm[i + 1]);
+    return 0.5 * (vminus + vplus);
+  }
+  if (ord == 3) {
+    const double dwe0 = 1.0 / 10.0, dwe1 = 6.0 / 10.0, dwe2 = 3.0 / 10.0;
+    const double d0 = 13.0 / 12.0, d1 = 1.0 / 4.0;
+    const double c0 = 1.0 / 3.0, c1 = 5.0 / 6.0, c2 = -1.0 / 6.0, c3 = -7.0 / 6.0, c4 = 11.0 / 6.0;
+    double a, b, bp0, bp1, bp2, bm0, bm1, bm2;
+    a = vp[i] - 2.0 * vp[i + 1] + vp[i + 2]; b = 3.0 * vp[i] - 4.0 * vp[i + 1] + vp[i + 2];
+    bp2 = bs * (d0 * (a * a) + d1 * (b * b));
+    a = vp[i - 1] - 2.0 * vp[i] + vp[i + 1]; b = vp[i - 1] - vp[i + 1];
+    bp1 = bs * (d0 * (a * a) + d1 * (b * b));
+    a = vp[i] - 2.0 * vp[i - 1] + vp[i - 2]; b = 3.0 * vp[i] - 4.0 * vp[i - 1] + vp[i - 2];
+    bp0 = bs * (d0 * (a * a) + d1 * (b * b));
+    a = vm[i + 1] - 2.0 * vm[i] + vm[i - 1]; b = 3.0 * vm[i + 1] - 4.0 * vm[i] + vm[i - 1];
+    bm2 = bs * (d0 * (a * a) + d1 * (b * b));
+    a = vm[i + 2] - 2.0 * vm[i + 1] + vm[i]; b = vm[i + 2] - vm[i];
+    bm1 = bs * (d0 * (a * a) + d1 * (b * b));
+    a = vm[i + 1] - 2.0 * vm[i + 2] + vm[i + 3]; b = 3.0 * vm[i + 1] - 4.0 * vm[i + 2] + vm[i + 3];
+    bm0 = bs * (d0 * (a * a) + d1 * (b * b));
+    double sp, sm;
+    if (version == 0) {
+      double t;
+      t = 0.000001 + bp0; bp0 = dwe0 / (t * t);
+      t = 0.000001 + bm0; bm0 = dwe0 / (t * t);
+      t = 0.000001 + bp1; bp1 = dwe1 / (t * t);
+      t = 0.000001 + bm1; bm1 = dwe1 / (t * t);
+      t = 0.000001 + bp2; bp2 = dwe2 / (t * t);
+      t = 0.000001 + bm2; bm2 = dwe2 / (t * t);
+    } else {
+      const double eps40 = 1.0e-40;
+      double tp = fabs(bp0 - bp2) + eps40, tm = fabs(bm0 - bm2) + eps40;
+      bp0 = (bp0 + eps40) / (bp0 + tp); bm0 = (bm0 + eps40) / (bm0 + tm);
+      bp1 = (bp1 + eps40) / (bp1 + tp); bm1 = (bm1 + eps40) / (bm1 + tm);
+      bp2 = (bp2 + eps40) / (bp2 + tp); bm2 = (bm2 + eps40) / (bm2 + tm);
+      bp0 = dwe0 / bp0; bm0 = dwe0 / bm0;
+      bp1 = dwe1 / bp1; bm1 = dwe1 / bm1;
+      bp2 = dwe2 / bp2; bm2 = dwe2 / bm2;
+    }
+    sp = bp0 + bp1 + bp2;
+    sm = bm0 + bm1 + bm2;
+    bp0 = bp0 / sp; bp1 = bp1 / sp; bp2 = bp2 / sp;
+    bm0 = bm0 / sm; bm1 = bm1 / sm; bm2 = bm2 / sm;
+    double vminus = bp2 * (c0 * vp[i] + c1 * vp[i + 1] + c2 * vp[i + 2]) +
+                    bp1 * (c2 * vp[i - 1] + c1 * vp[i] + c0 * vp[i + 1]) +
+                    bp0 * (c0 * vp[i - 2] + c3 * vp[i - 1] + c4 * vp[i]);
+    double vplus = bm2 * (c0 * vm[i + 1] + c1 * vm[i] + c2 * vm[i - 1]) +
+                   bm1 * (c2 * vm[i + 2] + c1 * vm[i + 1] + c0 * vm[i]) +
+                   bm0 * (c0 * vm[i + 3] + c3 * vm[i + 2] + c4 * vm[i + 1]);
+    return vminus + vplus;
+  }
+  // ord == 4: WENO-7
+  const double d1 = 1.0 / 36.0, d2 = 13.0 / 12.0, d3 = 781.0 / 720.0;
+  const double dwe[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0};
+  double bp[4], bm[4], a, b, e;
+  a = -11 * vp[i] + 18 * vp[i + 1] - 9 * vp[i + 2] + 2 * vp[i + 3];
+  b = 2 * vp[i] - 5 * vp[i + 1] + 4 * vp[i + 2] - vp[i + 3];
+  e = -vp[i] + 3 * vp[i + 1] - 3 * vp[i + 2] + vp[i + 3];
+  bp[3] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  a = -2 * vp[i - 1] - 3 * vp[i] + 6 * vp[i + 1] - vp[i + 2];
+  b = vp[i - 1] - 2 * vp[i] + vp[i + 1];
+  e = -vp[i - 1] + 3 * vp[i] - 3 * vp[i + 1] + vp[i + 2];
+  bp[2] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  a = vp[i - 2] - 6 * vp[i - 1] + 3 * vp[i] + 2 * vp[i + 1];
+  b = vp[i - 1] - 2 * vp[i] + vp[i + 1];
+  e = -vp[i - 2] + 3 * vp[i - 1] - 3 * vp[i] + vp[i + 1];
+  bp[1] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  a = -2 * vp[i - 3] + 9 * vp[i - 2] - 18 * vp[i - 1] + 11 * vp[i];
+  b = -vp[i - 3] + 4 * vp[i - 2] - 5 * vp[i - 1] + 2 * vp[i];
+  e = -vp[i - 3] + 3 * vp[i - 2] - 3 * vp[i - 1] + vp[i];
+  bp[0] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  a = -11 * vm[i + 1] + 18 * vm[i] - 9 * vm[i - 1] + 2 * vm[i - 2];
+  b = 2 * vm[i + 1] - 5 * vm[i] + 4 * vm[i - 1] - vm[i - 2];
+  e = -vm[i + 1] + 3 * vm[i] - 3 * vm[i - 1] + vm[i - 2];
+  bm[3] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  a = -2 * vm[i + 2] - 3 * vm[i + 1] + 6 * vm[i] - vm[i - 1];
+  b = vm[i + 2] - 2 * vm[i + 1] + vm[i];
+  e = -vm[i + 2] + 3 * vm[i + 1] - 3 * vm[i] + vm[i - 1];
+  bm[2] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  a = vm[i + 3] - 6 * vm[i + 2] + 3 * vm[i + 1] + 2 * vm[i];
+  b = vm[i + 2] - 2 * vm[i + 1] + vm[i];
+  e = -vm[i + 3] + 3 * vm[i + 2] - 3 * vm[i + 1] + vm[i];
+  bm[1] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  a = -2 * vm[i + 4] + 9 * vm[i + 3] - 18 * vm[i + 2] + 11 * vm[i + 1];
+  b = -vm[i + 4] + 4 * vm[i + 3] - 5 * vm[i + 2] + 2 * vm[i + 1];
+  e = -vm[i + 4] + 3 * vm[i + 3] - 3 * vm[i + 2] + vm[i + 1];
+  bm[0] = d1 * (a * a) + d2 * (b * b) + d3 * (e * e);
+  double sp = 0.0, sm = 0.0;
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    double t = 0.000001 + bs * bp[l]; bp[l] = dwe[l] / (t * t);
+    t = 0.000001 + bs * bm[l]; bm[l] = dwe[l] / (t * t);
+    sp = sp + bp[l]; sm = sm + bm[l];
+  }
+#pragma unroll
+  for (int l = 0; l < 4; l++) { bp[l] = bp[l] / sp; bm[l] = bm[l] / sm; }
+  double vminus = bp[3] * (6 * vp[i] + 26 * vp[i + 1] - 10 * vp[i + 2] + 2 * vp[i + 3]) +
+                  bp[2] * (-2 * vp[i - 1] + 14 * vp[i] + 14 * vp[i + 1] - 2 * vp[i + 2]) +
+                  bp[1] * (2 * vp[i - 2] - 10 * vp[i - 1] + 26 * vp[i] + 6 * vp[i + 1]) +
+                  bp[0] * (-6 * vp[i - 3] + 26 * vp[i - 2] - 46 * vp[i - 1] + 50 * vp[i]);
+  double vplus = bm[3] * (6 * vm[i + 1] + 26 * vm[i] - 10 * vm[i - 1] + 2 * vm[i - 2]) +
+                 bm[2] * (-2 * vm[i + 2] + 14 * vm[i + 1] + 14 * vm[i] - 2 * vm[i - 1]) +
+                 bm[1] * (2 * vm[i + 3] - 10 * vm[i + 2] + 26 * vm[i + 1] + 6 * vm[i]) +
+                 bm[0] * (-6 * vm[i + 4] + 26 * vm[i + 3] - 46 * vm[i + 2] + 50 * vm[i + 1]);
+  return (vminus + vplus) / 24.0;
+}
+
+#define WMAX 8   // 2 * max weno_scheme
+
+// Central KEEP(n) face flux (kernels_gpu.F90:145-337 and the y/z copies).
+template <int NS, int DIR>
+__device__ __forceinline__ void central_flux(const DevCtx &c, const double *__restrict__ wa, long long p, long long st,
+                                             bool fz, double *fh) {
+  const DevGrid &g = c.g;
+  const int J_U = NS + 1, J_V = NS + 2, J_W = NS + 3, J_H = NS + 4, J_P = NS + 6, J_R = NS + 11;
+  const int Jn = J_U + DIR;
+  int lmax = c.p.ep_order / 2;
+  if (lmax < 1) lmax = 1;
+  const int nkeep = c.p.nkeep;
+#pragma unroll 1
+  for (int lsp = 1; lsp <= NS; lsp++) {
+    double ft1 = 0.0;
+    for (int l = 1; l <= lmax; l++) {
+      double uvs1 = 0.0;
+      for (int m = 0; m <= l - 1; m++) {
+        long long a = p - m * st, b = p + (l - m) * st;
+        double rhoi = FG(wa, a, J_R), uui = FG(wa, a, Jn), yyi = FG(wa, a, lsp);
+        double rhoip = FG(wa, b, J_R), uuip = FG(wa, b, Jn), yyip = FG(wa, b, lsp);
+        double rhom = rhoi + rhoip, drhof;
+        if (nkeep <= 0) {
+          drhof = 1.0;
+        } else {
+          double drho = 2.0 * (rhoip - rhoi) / rhom;
+          double t = (0.5 * drho) * (0.5 * drho), t2 = t;
+          double sumden = 1.0 + t / 3.0;
+          for (int n = 2; n <= nkeep; n++) { int n2 = 2 * n; t = t2 * t; sumden = sumden + t / (1.0 + n2); }
+          drhof = 1.0 / sumden;
+        }
+        double uv_part = (uui + uuip) * rhom * drhof;
+        uvs1 = uvs1 + uv_part * (yyi + yyip);
+      }
+      ft1 = ft1 + c.p.cd1[l][lmax] * uvs1;
+    }
+    double fh1 = 0.25 * ft1;
+    fh[lsp - 1] = fz ? 0.0 : fh1;
+  }
+  double ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
+  for (int l = 1; l <= lmax; l++) {
+    double uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs6 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0;
+    for (int m = 0; m <= l - 1; m++) {
+      long long a = p - m * st, b = p + (l - m) * st;
+      double rhoi = FG(wa, a, J_R), uui = FG(wa, a, J_U), vvi = FG(wa, a, J_V), wwi = FG(wa, a, J_W);
+      double enti = FG(wa, a, J_H), ppi = FG(wa, a, J_P);
+      double rhoip = FG(wa, b, J_R), uuip = FG(wa, b, J_U), vvip = FG(wa, b, J_V), wwip = FG(wa, b, J_W);
+      double entip = FG(wa, b, J_H), ppip = FG(wa, b, J_P);
+      double uni = DIR == 0 ? uui : (DIR == 1 ? vvi : wwi);
+      double unip = DIR == 0 ? uuip : (DIR == 1 ? vvip : wwip);
+      double rhom = rhoi + rhoip;
+      if (nkeep >= 0) {
+        double eei = enti - ppi / rhoi - 0.5 * (uui * uui + vvi * vvi + wwi * wwi);
+        double eeip = entip - ppip / rhoip - 0.5 * (uuip * uuip + vvip * vvip + wwip * wwip);
+        double eem = eei + eeip, drhof, deef;
+        if (nkeep == 0) {
+          drhof = 1.0; deef = 1.0;
+        } else {
+          double drho = 2.0 * (rhoip - rhoi) / rhom;
+          double dee = 2.0 * (eeip - eei) / eem;
+          double tr = (0.5 * drho) * (0.5 * drho), te = (0.5 * dee) * (0.5 * dee);
+          double tr2 = tr, te2 = te;
+          double sdr = 1.0 + tr / 3.0, sde = 1.0 + te, sne = 1.0 + te / 3.0;
+          for (int n = 2; n <= nkeep; n++) {
+            int n2 = 2 * n;
+            tr = tr2 * tr; te = te2 * te;
+            sdr = sdr + tr / (1.0 + n2);
+            sde = sde + te;
+            sne = sne + te / (1.0 + n2);
+          }
+          drhof = 1.0 / sdr;
+          deef = sne / sde;
+        }
+        double uv_part = (uni + unip) * rhom * drhof;
+        uvs2 = uvs2 + uv_part * (uui + uuip);
+        uvs3 = uvs3 + uv_part * (vvi + vvip);
+        uvs4 = uvs4 + uv_part * (wwi + wwip);
+        uvs5_i = uvs5_i + uv_part * eem * deef;
+        uvs5_k = uvs5_k + uv_part * (uui * uuip + vvi * vvip + wwi * wwip);
+        uvs5_p = uvs5_p + 4.0 * (uni * ppip + unip * ppi);
+        uvs6 = uvs6 + (2.0) * (ppi + ppip);
+      } else {
+        double uv_part = (uni + unip) * rhom;
+        uvs2 = uvs2 + uv_part * (uui + uuip);
+        uvs3 = uvs3 + uv_part * (vvi + vvip);
+        uvs4 = uvs4 + uv_part * (wwi + wwip);
+        uvs5 = uvs5 + uv_part * (enti + entip);
+        uvs6 = uvs6 + (2.0) * (ppi + ppip);
+      }
+    }
+    double cl = c.p.cd1[l][lmax];
+    ft2 = ft2 + cl * uvs2;
+    ft3 = ft3 + cl * uvs3;
+    ft4 = ft4 + cl * uvs4;
+    ft5 = ft5 + cl * (nkeep >= 0 ? (uvs5_i + uvs5_k + uvs5_p) : uvs5);
+    ft6 = ft6 + cl * uvs6;
+  }
+  double fm0 = 0.25 * ft2, fm1 = 0.25 * ft3, fm2 = 0.25 * ft4, fh5 = 0.25 * ft5;
+  if (fz) { fm0 = fm1 = fm2 = fh5 = 0.0; }
+  if (DIR == 0) fm0 = fm0 + 0.5 * ft6;
+  if (DIR == 1) fm1 = fm1 + 0.5 * ft6;
+  if (DIR == 2) fm2 = fm2 + 0.5 * ft6;
+  fh[NS] = fm0; fh[NS + 1] = fm1; fh[NS + 2] = fm2; fh[NS + 3] = fh5;
+}
+
+// Roe state (compute_roe_average, kernels_gpu.F90:2986-3295) between p and q.
+template <int NS>
+__device__ __forceinline__ void roe_state(const DevCtx &c, const double *__restrict__ wa, long long p, long long q,
+                                          double &b1, double &b2, double &b3, double &rho_r, double &cr, double &ci,
+                                          double &hr, double vel[3], double *yr, double *prhoi) {
+  const DevGrid &g = c.g;
+  const DevTab &t = c.t;
+  const int J_U = NS + 1, J_V = NS + 2, J_W = NS + 3, J_H = NS + 4, J_P = NS + 6, J_R = NS + 11;
+  double rho = FG(wa, p, J_R), uu = FG(wa, p, J_U), vv = FG(wa, p, J_V), ww = FG(wa, p, J_W);
+  double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+  double h = FG(wa, p, J_H), pp = FG(wa, p, J_P);
+  double ee = h - pp / rho - qq;
+  double rho_L = rho, ee_L = ee;
+  double rhop = FG(wa, q, J_R), up = FG(wa, q, J_U), vp = FG(wa, q, J_V), wp = FG(wa, q, J_W);
+  double qqp = 0.5 * (up * up + vp * vp + wp * wp);
+  double hp = FG(wa, q, J_H), ppp = FG(wa, q, J_P);
+  double eep = hp - ppp / rhop - qqp;
+  double r = sqrt(rhop / rho);
+  rho = r * rho_L;
+  double rp1 = 1.0 / (r + 1.0);
+  uu = (r * up + uu) * rp1;
+  vv = (r * vp + vv) * rp1;
+  ww = (r * wp + ww) * rp1;
+  h = (r * hp + h) * rp1;
+  qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+  ee = (r * eep + ee) * rp1;
+  double p_over_rho = h - ee - qq;
+  double rm = 0.0, drho[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    double yy = FG(wa, p, k + 1), yyp = FG(wa, q, k + 1);
+    drho[k] = rhop * yyp - rho_L * yy;
+    yy = (r * yyp + yy) * rp1;
+    rm = rm + ldg(t.rgas + k) * yy;
+    yr[k] = yy;
+  }
+  double told = p_over_rho / rm;
+  double tt = temp_from_e<NS>(t, c.p, ee, told, yr);
+  double cploc = mix_cp<NS>(t, tt, yr);
+  double gamloc = cploc / (cploc - rm);
+  double gm1loc = gamloc - 1.0;
+  double p_e = rho * gm1loc;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    double eei = species_poly_int(t, t.cv, tt, k + 1);
+    prhoi[k] = ldg(t.rgas + k) * tt + gm1loc * (ee - eei);
+  }
+  double etot = ee + qq;
+  double dp_SLV = ppp - pp, de_SLV = eep - ee_L;
+  double pede = p_e * de_SLV;
+  double dp_err = dp_SLV - pede;
+  double den = pede * pede;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    double pr = prhoi[k] * drho[k];
+    dp_err = dp_err - pr;
+    den = den + pr * pr;
+  }
+  double dpfact = dp_err / dmax_(den, 0.000001);
+  p_e = p_e * (1.0 + pede * dpfact);
+#pragma unroll
+  for (int k = 0; k < NS; k++) prhoi[k] = prhoi[k] * (1.0 + prhoi[k] * drho[k] * dpfact);
+  double cc = p_over_rho / rho * p_e;
+#pragma unroll
+  for (int k = 0; k < NS; k++) cc = cc + yr[k] * prhoi[k];
+  cr = sqrt(cc);
+  ci = 1.0 / cr;
+  b3 = etot;
+  b2 = p_e / (rho * cc);
+  b1 = -b2 * (etot - 2.0 * qq);
+  rho_r = rho;
+  hr = h;
+  vel[0] = uu; vel[1] = vv; vel[2] = ww;
+}
+
+// Characteristic (Roe) WENO face flux with LLF splitting (kernels_gpu.F90:338-423).
+template <int NS, int DIR>
+__device__ __noinline__ void weno_char_flux(const DevCtx &c, const double *__restrict__ wa, long long p, long long st,
+                                            double *fh) {
+  const DevGrid &g = c.g;
+  const int NV = NS + 4;
+  const int J_U = NS + 1, J_H = NS + 4, J_P = NS + 6, J_C = NS + 7, J_R = NS + 11;
+  const int T1 = DIR == 0 ? 1 : 0, T2 = DIR == 2 ? 1 : 2;
+  const int ws = c.p.weno_scheme, wsz = 2 * ws;
+  double b1, b2, b3, rr, cr, ci, hr, vr[3], yr[NS], prhoi[NS];
+  roe_state<NS>(c, wa, p, p + st, b1, b2, b3, rr, cr, ci, hr, vr, yr, prhoi);
+  const double un = vr[DIR], ut1 = vr[T1], ut2 = vr[T2];
+  const double cci = ci * ci;
+  double b1i[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) b1i[k] = b1 + prhoi[k] * cci;
+  // LLF eigenvalue bounds over the stencil (:345-358)
+  double ev1 = -1.0, ev2 = -1.0, ev4 = -1.0;
+  for (int l = 1; l <= wsz; l++) {
+    long long q = p + (l - ws) * st;
+    double u = FG(wa, q, J_U + DIR), cq = FG(wa, q, J_C);
+    ev1 = dmax_(fabs(u - cq), ev1);
+    ev2 = dmax_(fabs(u), ev2);
+    ev4 = dmax_(fabs(u + cq), ev4);
+  }
+  // per-point scalars
+  double Qw[WMAX + 1], Qf[WMAX + 1], sw[WMAX + 1], sf[WMAX + 1];
+  double Wn[WMAX + 1], Fn[WMAX + 1], Wt1[WMAX + 1], Ft1[WMAX + 1], Wt2[WMAX + 1], Ft2[WMAX + 1];
+  double rl[WMAX + 1], rul[WMAX + 1];
+  for (int l = 1; l <= wsz; l++) {
+    long long q = p + (l - ws) * st;
+    double rho = FG(wa, q, J_R), u0 = FG(wa, q, J_U), u1 = FG(wa, q, J_U + 1), u2 = FG(wa, q, J_U + 2);
+    double h = FG(wa, q, J_H), pp = FG(wa, q, J_P);
+    double vel[3] = {u0, u1, u2};
+    double rhou = rho * vel[DIR];
+    double Sw = 0.0, Sf = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      double y = FG(wa, q, k + 1);
+      double wk = rho * y, fk = rhou * y;
+      Sw = Sw + b1i[k] * wk;
+      Sf = Sf + b1i[k] * fk;
+      s1 = s1 + wk;
+      s2 = s2 + fk;
+    }
+    double wm0 = rho * u0, wm1 = rho * u1, wm2 = rho * u2;
+    double fm0 = u0 * rhou, fm1 = u1 * rhou, fm2 = u2 * rhou;
+    if (DIR == 0) fm0 = fm0 + pp;
+    if (DIR == 1) fm1 = fm1 + pp;
+    if (DIR == 2) fm2 = fm2 + pp;
+    double wE = rho * h - pp, fE = h * rhou;
+    Qw[l] = Sw - b2 * (vr[0] * wm0 + vr[1] * wm1 + vr[2] * wm2) + b2 * wE;
+    Qf[l] = Sf - b2 * (vr[0] * fm0 + vr[1] * fm1 + vr[2] * fm2) + b2 * fE;
+    sw[l] = s1; sf[l] = s2;
+    double wmv[3] = {wm0, wm1, wm2}, fmv[3] = {fm0, fm1, fm2};
+    Wn[l] = wmv[DIR]; Fn[l] = fmv[DIR];
+    Wt1[l] = wmv[T1]; Ft1[l] = fmv[T1];
+    Wt2[l] = wmv[T2]; Ft2[l] = fmv[T2];
+    rl[l] = rho; rul[l] = rhou;
+  }
+  // betascale (wenorec_1d, :2372-2381)
+  const double u0 = c.p.u0, rho0 = c.p.rho0;
+  const double r2u2 = rho0 * rho0 * (u0 * u0), r2u4 = r2u2 * (u0 * u0);
+  const double bsA = 1.0 / r2u2, bsB = 1.0 / r2u4;
+  int ord = ws < 1 ? 1 : ws;
+  double fi[NV];
+  double vp[WMAX + 1], vm[WMAX + 1];
+  // characteristic 1 (u - c) and NS+4 (u + c)
+#pragma unroll 1
+  for (int side = 0; side < 2; side++) {
+    double sg = side == 0 ? 1.0 : -1.0, ev = side == 0 ? ev1 : ev4;
+    for (int l = 1; l <= wsz; l++) {
+      double wc = 0.5 * (Qw[l] + sg * ci * (un * sw[l] - Wn[l]));
+      double gc = 0.5 * (Qf[l] + sg * ci * (un * sf[l] - Fn[l]));
+      double cc = 0.5 * (gc + ev * wc);
+      vp[l] = cc; vm[l] = gc - cc;
+    }
+    double v = weno_rec(vp, vm, ws, ord, c.p.weno_version, bsA);
+    if (side == 0) fi[0] = v; else fi[NV - 1] = v;
+  }
+  // species characteristics 1+lsp
+#pragma unroll 1
+  for (int k = 0; k < NS; k++) {
+    for (int l = 1; l <= wsz; l++) {
+      long long q = p + (l - ws) * st;
+      double y = FG(wa, q, k + 1);
+      double wc = rl[l] * y - yr[k] * Qw[l];
+      double gc = rul[l] * y - yr[k] * Qf[l];
+      double cc = 0.5 * (gc + ev2 * wc);
+      vp[l] = cc; vm[l] = gc - cc;
+    }
+    fi[1 + k] = weno_rec(vp, vm, ws, ord, c.p.weno_version, bsA);
+  }
+  // tangential characteristics NS+2, NS+3
+#pragma unroll 1
+  for (int side = 0; side < 2; side++) {
+    double ut = side == 0 ? ut1 : ut2;
+    for (int l = 1; l <= wsz; l++) {
+      double wc = (side == 0 ? Wt1[l] : Wt2[l]) - ut * sw[l];
+      double gc = (side == 0 ? Ft1[l] : Ft2[l]) - ut * sf[l];
+      double cc = 0.5 * (gc + ev2 * wc);
+      vp[l] = cc; vm[l] = gc - cc;
+    }
+    fi[NS + 1 + side] = weno_rec(vp, vm, ws, ord, c.p.weno_version, bsB);
+  }
+  // back projection with the reference's summation order (eigenvectors_*, :415-420)
+  const double f0 = fi[0], f4 = fi[NV - 1];
+#pragma unroll
+  for (int k = 0; k < NS; k++) fh[k] = (yr[k] * f0 + fi[1 + k]) + yr[k] * f4;
+  double an = (un - cr) * f0, a1 = ut1 * f0, a2 = ut2 * f0, aE = (hr - un * cr) * f0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    double fk = fi[1 + k];
+    an = an + un * fk;
+    a1 = a1 + ut1 * fk;
+    a2 = a2 + ut2 * fk;
+    aE = aE + (b3 - prhoi[k] / b2 * cci) * fk;
+  }
+  a1 = a1 + fi[NS + 1];
+  a2 = a2 + fi[NS + 2];
+  aE = aE + ut1 * fi[NS + 1];
+  aE = aE + ut2 * fi[NS + 2];
+  an = an + (un + cr) * f4;
+  a1 = a1 + ut1 * f4;
+  a2 = a2 + ut2 * f4;
+  aE = aE + (hr + un * cr) * f4;
+  fh[NS + DIR] = an;
+  fh[NS + T1] = a1;
+  fh[NS + T2] = a2;
+  fh[NS + 3] = aE;
+}
+
+// Component-wise Rusanov WENO face flux (kernels_gpu.F90:671-725).
+template <int NS, int DIR>
+__device__ __noinline__ void weno_rusanov_flux(const DevCtx &c, const double *__restrict__ wa, long long p, long long st,
+                                               double *fh) {
+  const DevGrid &g = c.g;
+  const int J_U = NS + 1, J_H = NS + 4, J_P = NS + 6, J_C = NS + 7, J_R = NS + 11;
+  const int ws = c.p.weno_scheme, wsz = 2 * ws;
+  int ord = ws < 1 ? 1 : ws;
+  double evmax = -1.0;
+  for (int l = 1; l <= wsz; l++) {
+    long long q = p + (l - ws) * st;
+    double u = FG(wa, q, J_U + DIR), cq = FG(wa, q, J_C);
+    evmax = dmax_(dmax_(fabs(u - cq), fabs(u + cq)), evmax);
+  }
+  const double u0 = c.p.u0, rho0 = c.p.rho0, u02 = u0 * u0;
+  const double r2u2 = rho0 * rho0 * u02, r2u4 = r2u2 * u02, r2u4i = 1.0 / r2u4;
+  double vp[WMAX + 1], vm[WMAX + 1];
+#pragma unroll 1
+  for (int m = 0; m < NS + 4; m++) {
+    for (int l = 1; l <= wsz; l++) {
+      long long q = p + (l - ws) * st;
+      double rho = FG(wa, q, J_R), un = FG(wa, q, J_U + DIR);
+      double rhou = rho * un, rhoevm = rho * evmax, evm, cc;
+      if (m < NS) {
+        double yy = FG(wa, q, m + 1);
+        evm = rhou * yy;
+        cc = 0.5 * (evm + rhoevm * yy);
+      } else if (m < NS + 3) {
+        int d = m - NS;
+        double vd = FG(wa, q, J_U + d);
+        evm = (d == DIR) ? vd * rhou + FG(wa, q, J_P) : vd * rhou;
+        cc = 0.5 * (evm + rhoevm * vd);
+      } else {
+        double h = FG(wa, q, J_H), pp = FG(wa, q, J_P);
+        evm = h * rhou;
+        cc = 0.5 * (evm + evmax * (rho * h - pp));
+      }
+      vp[l] = cc; vm[l] = evm - cc;
+    }
+    double bs = m < NS ? 1.0 / r2u2 : (m < NS + 3 ? r2u4i : r2u4i / u02);
+    fh[m] = weno_rec(vp, vm, ws, ord, c.p.weno_version, bs);
+  }
+}
+
+// Hybrid face flux: Ducros test over the WENO stencil, then central or upwind.
+template <int NS, int DIR>
+__device__ __forceinline__ void face_flux(const DevCtx &c, const double *__restrict__ wa, long long p, long long st,
+                                          int face, int nmax, double *fh) {
+  const DevGrid &g = c.g;
+  const int J_DUC = NS + 9;
+  const int ws = c.p.weno_scheme;
+  bool shk = false;
+  for (int s = -ws + 1; s <= ws; s++) shk |= (FG(wa, p + s * st, J_DUC) > c.p.sensor_threshold);
+  if (!shk) {
+    bool fz = (face == 0 && c.p.fzf[2 * DIR] == 1) || (face == nmax && c.p.fzf[2 * DIR + 1] == 1);
+    central_flux<NS, DIR>(c, wa, p, st, fz, fh);
+  } else if (c.p.flux_splitting == 1) {
+    weno_rusanov_flux<NS, DIR>(c, wa, p, st, fh);
+  } else {
+    weno_char_flux<NS, DIR>(c, wa, p, st, fh);
+  }
+}
+
+// x sweep: faces through shared memory
+template <int NS>
+__global__ void __launch_bounds__(128) k_euler_x(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl,
+                                                 int nmin, int nmax, int overwrite) {
+  const DevGrid &g = c.g;
+  const int NV = NS + 4;
+  __shared__ double sf[NV][128];
+  int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  int f0 = nmin - 1 + blockIdx.x * 127;
+  int f = f0 + threadIdx.x;
+  double fh[NV];
+  if (f <= nmax) {
+    long long p = gidx(g, f, j, k);
+    face_flux<NS, 0>(c, wa, p, 1, f, g.nx, fh);
+#pragma unroll
+    for (int m = 0; m < NV; m++) sf[m][threadIdx.x] = fh[m];
+  }
+  __syncthreads();
+  int i = f;
+  if (threadIdx.x >= 1 && i <= nmax) {
+    long long q = fidx(g, i, j, k);
+    double met = ldg(g.dcsidx + i - 1);
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      double d = (sf[m][threadIdx.x] - sf[m][threadIdx.x - 1]) * met;
+      FI(fl, q, m + 1) = overwrite ? d : FI(fl, q, m + 1) + d;
+    }
+  }
+}
+
+// y / z sweeps: march along the sweep
+template <int NS, int DIR>
+__global__ void __launch_bounds__(128) k_euler_yz(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl,
+                                                  int nmin, int nmax, int chunk, int overwrite) {
+  const DevGrid &g = c.g;
+  const int NV = NS + 4;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > g.nx) return;
+  int tr = blockIdx.y + 1;                 // k for the y sweep, j for the z sweep
+  int c0 = nmin + blockIdx.z * chunk;
+  int c1 = min(c0 + chunk - 1, nmax);
+  long long st = DIR == 1 ? (long long)g.nxg : (long long)g.nxg * g.nyg;
+  const double *met = DIR == 1 ? g.detady : g.dzitdz;
+  int nsw = DIR == 1 ? g.ny : g.nz;
+  double prev[NV], cur[NV];
+  {
+    int f = c0 - 1;
+    long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
+    face_flux<NS, DIR>(c, wa, p, st, f, nsw, prev);
+  }
+  for (int f = c0; f <= c1; f++) {
+    long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
+    face_flux<NS, DIR>(c, wa, p, st, f, nsw, cur);
+    long long q = DIR == 1 ? fidx(g, i, f, tr) : fidx(g, i, tr, f);
+    double mt = ldg(met + f - 1);
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      double d = (cur[m] - prev[m]) * mt;
+      FI(fl, q, m + 1) = overwrite ? d : FI(fl, q, m + 1) + d;
+      prev[m] = cur[m];
+    }
+  }
+}
+
+template <int NS>
+static int euler_t(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl, int nmin, int nmax, int ow) {
+  const DevGrid &g = c.g;
+  if (nmax - nmin < 0) return STX_OK;
+  if (2 * c.p.weno_scheme > WMAX) return STX_E_UNSUPPORTED;
+  if (dir == 0) {
+    int ncell = nmax - nmin + 1;
+    dim3 grid((ncell + 126) / 127, g.ny, g.nz);
+    k_euler_x<NS><<<grid, 128, 0, s>>>(c, wa, fl, nmin, nmax, ow);
+  } else {
+    int chunk = 16;
+    int ncell = nmax - nmin + 1;
+    dim3 grid((g.nx + 127) / 128, dir == 1 ? g.nz : g.ny, (ncell + chunk - 1) / chunk);
+    if (dir == 1) k_euler_yz<NS, 1><<<grid, 128, 0, s>>>(c, wa, fl, nmin, nmax, chunk, ow);
+    else k_euler_yz<NS, 2><<<grid, 128, 0, s>>>(c, wa, fl, nmin, nmax, chunk, ow);
+  }
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_euler(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl, int nmin, int nmax, int ow) {
+  switch (c.t.ns) {
+#define X(N) case N: return euler_t<N>(c, s, dir, wa, fl, nmin, nmax, ow);
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
+}

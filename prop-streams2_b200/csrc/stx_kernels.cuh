@@ -1,0 +1,25 @@
+// stx_kernels.cuh -- launchers shared between the translation units of libstx.so.
+#pragma once
+#include "stx_common.cuh"
+
+int launch_eval_aux(const DevCtx &c, cudaStream_t s, double *w, double *wa, int i0, int i1, int j0, int j1, int k0, int k1);
+int launch_eval_aux2(const DevCtx &c, cudaStream_t s, double *wa);
+int launch_bcextr_var(const DevCtx &c, cudaStream_t s, double *v);
+int launch_bcswap(const DevCtx &c, cudaStream_t s, double *f, int nvar, const int *periodic);
+int launch_bc_face(const DevCtx &c, cudaStream_t s, double *w, int ilat, int tag, const double *winf);
+int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt);
+int launch_update_flux(const DevCtx &c, cudaStream_t s, const double *fl, double *fln, const double *fl_sav, double gamdt);
+int launch_copy(const DevCtx &c, cudaStream_t s, const double *a, double *b);
+int launch_update_field(const DevCtx &c, cudaStream_t s, double *w, const double *fl, double *fln, const double *fl_sav,
+                        const int32_t *mask, double gamdt, int fused);
+int launch_compute_dt(const DevCtx &c, cudaStream_t s, const double *wa, const int32_t *mask, unsigned long long *out9);
+
+int launch_euler(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl, int nmin, int nmax, int overwrite);
+int launch_visflx(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl);
+int launch_visflx_reduced(const DevCtx &c, cudaStream_t s, const double *wa, double *fl);
+
+int launch_rok4(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
+                double t0, double t1, int simpler, unsigned int *counter);
+int launch_rosenbrock(const DevCtx &c, cudaStream_t s, double *w, double *wa, double dttry, double t0, double t1,
+                      unsigned int *counter);
+int launch_chem_explicit(const DevCtx &c, cudaStream_t s, double *w, double *wa, double *fl);

@@ -1,0 +1,131 @@
+"""Device-side equation object: the B200 drop-in for the reference's
+``equation_multideal_gpu_object`` (src/multideal/multideal_gpu.F90:164-211).
+
+Fields live in HBM as torch tensors in the reference's SoA layout; every
+kernel runs from ``libstx.so`` through its C ABI on the current torch stream.
+There is no CPU path: if the CUDA library is missing, construction fails.
+Method names follow the reference (``update_ghost``, ``compute_aux``,
+``compute_dt``, ``rk_sync``, ``advance_solution``, ``run``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+import torch
+
+from .native import StxFields, check, load_stx
+
+
+def _p(t: Optional[torch.Tensor]):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+class Solver:
+    def __init__(self, case, device: str = "cuda"):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the stx solver needs a CUDA device (there is no CPU fallback)")
+        self.lib = load_stx()
+        self.case = case
+        self.device = torch.device(device)
+        torch.cuda.set_device(self.device)
+        self._par, self._tab, self._grid = case.params_struct(), case.tables_struct(), case.grid_struct()
+        ctx = C.c_void_p()
+        check(self.lib.stx_ctx_create(C.byref(self._par), C.byref(self._tab), C.byref(self._grid), C.byref(ctx)),
+              "stx_ctx_create")
+        self.ctx = ctx
+        nv = case.nv
+        self.w = torch.from_numpy(case.w).to(self.device).contiguous()
+        self.w_aux = torch.from_numpy(case.w_aux).to(self.device).contiguous()
+        shp = (nv, case.nz, case.ny, case.nx)
+        self.fl = torch.zeros(shp, dtype=torch.float64, device=self.device)
+        self.fln = torch.zeros(shp, dtype=torch.float64, device=self.device)
+        self.fl_sav = torch.zeros(shp, dtype=torch.float64, device=self.device)
+        self.fields = StxFields(self.w.data_ptr(), self.w_aux.data_ptr(), self.fl.data_ptr(), self.fln.data_ptr(),
+                                self.fl_sav.data_ptr(), None)
+        self.time = 0.0
+        self.dt = 0.0
+        self.icyc = 0
+
+    # ------------------------------------------------------------------ plumbing
+    @property
+    def stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.stx_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def aux_slot(self, j: int) -> C.c_void_p:
+        return C.c_void_p(self.w_aux[j].data_ptr())
+
+    def status(self, reset: bool = True) -> int:
+        b = C.c_uint32()
+        check(self.lib.stx_status(self.ctx, self.stream, C.byref(b), 1 if reset else 0), "stx_status")
+        return b.value
+
+    # ------------------------------------------------------------------ reference-named calls
+    def update_ghost(self, do_swap: int = 1):
+        check(self.lib.stx_update_ghost(self.ctx, self.stream, _p(self.w), do_swap), "update_ghost")
+
+    def compute_aux(self, central: int = 1, ghost: int = 1):
+        check(self.lib.stx_compute_aux(self.ctx, self.stream, _p(self.w), _p(self.w_aux), central, ghost), "compute_aux")
+
+    def compute_dt(self) -> float:
+        cfl = self.case.cfl
+        if cfl < 0:
+            self.dt = -cfl
+        else:
+            out = (C.c_double * 9)()
+            check(self.lib.stx_compute_dt(self.ctx, self.stream, _p(self.w_aux), None, out), "compute_dt")
+            self.dt = cfl / max(out)
+        return self.dt
+
+    def rk_sync(self, dt: Optional[float] = None, simpler: int = 0):
+        check(self.lib.stx_rk_sync(self.ctx, self.stream, C.byref(self.fields), self.dt if dt is None else dt, simpler),
+              "rk_sync")
+
+    def advance_solution(self):
+        check(self.lib.stx_advance_solution(self.ctx, self.stream, C.byref(self.fields), self.dt, self.time),
+              "advance_solution")
+
+    def prepare(self):
+        """Start of ``run`` (multideal_gpu.F90:1687-1727)."""
+        c = self.case
+        self.update_ghost(1)
+        self.compute_aux(1, 1)
+        check(self.lib.stx_bcextr_var(self.ctx, self.stream, self.aux_slot(c.J("DIV"))), "bcextr_var")
+        check(self.lib.stx_bcswap(self.ctx, self.stream, self.aux_slot(c.J("DIV")), 1), "bcswap_var")
+        check(self.lib.stx_bcswap(self.ctx, self.stream, self.aux_slot(c.J("DUC")), 1), "bcswap_var")
+        self.fl.zero_()
+        self.compute_dt()
+
+    def step(self, recompute_dt: bool = True):
+        """One iteration of the reference's ``integration`` loop (:1745-1806), no output."""
+        self.icyc += 1
+        if recompute_dt and self.icyc % self.case.iter_dt_recompute == 0:
+            self.compute_aux(1, 0)
+            self.compute_dt()
+        self.advance_solution()
+        self.compute_aux(1, 0)
+        self.time = self.time + self.dt
+
+    def run(self, num_iter: int):
+        self.prepare()
+        for _ in range(num_iter):
+            self.step()
+
+    # ------------------------------------------------------------------ host views
+    def host_w(self) -> np.ndarray:
+        return self.w.cpu().numpy()
+
+    def host_w_aux(self) -> np.ndarray:
+        return self.w_aux.cpu().numpy()
