@@ -183,6 +183,27 @@ int stx_advance_solution(stx_ctx *ctx, void *stream, const stx_fields *f, double
 /* Device status word (OR of STX_ST_* bits since the last reset); synchronises the stream. */
 int stx_status(stx_ctx *ctx, void *stream, uint32_t *bits, int reset);
 
+/* Instrumentation: kernel classes whose launches are counted and, while
+ * profiling is on, timed with CUDA events recorded on the launching stream. */
+#define STX_K_EVAL_AUX 0   /* eval_aux */
+#define STX_K_DUCROS   1   /* eval_aux2 */
+#define STX_K_GHOST    2   /* bcswap, bcextr_var, update_ghost faces */
+#define STX_K_EULER    3   /* fused convective flux + divergence */
+#define STX_K_VISC     4   /* viscous / diffusion fluxes, both modes */
+#define STX_K_RK       5   /* RK bookkeeping */
+#define STX_K_CHEM     6   /* Rosenbrock / ROK4 / explicit source */
+#define STX_K_DT       7   /* CFL reduction */
+#define STX_NK         8
+typedef struct stx_kprof {
+  int64_t launches;    /* kernel launches since the last stx_profile_enable */
+  int64_t timed;       /* entry-point calls timed with events */
+  double  ms;          /* summed event time of the timed calls */
+} stx_kprof;
+/* Reset the counters; on != 0 also records events around every launch. */
+int stx_profile_enable(stx_ctx *ctx, int on);
+/* Synchronises the device and fills out[STX_NK]. */
+int stx_profile_read(stx_ctx *ctx, stx_kprof *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,39 @@ struct stx_ctx {
   unsigned long long *dt_d;       // the nine CFL maxima
   std::vector<void *> allocs;
   int device;
+  // instrumentation (stx_profile_*)
+  int prof_on;
+  long long launches[STX_NK];
+  std::vector<cudaEvent_t> ev[STX_NK];   // begin/end pairs
+  size_t ev_used[STX_NK];
 };
+
+namespace {
+// Counts the kernels an entry point launches and, with profiling on, brackets
+// them with a pair of events on the launching stream.
+struct Prof {
+  stx_ctx *c;
+  cudaStream_t s;
+  int cls;
+  cudaEvent_t e1 = nullptr;
+  Prof(stx_ctx *c_, cudaStream_t s_, int cls_, int nlaunch) : c(c_), s(s_), cls(cls_) {
+    c->launches[cls] += nlaunch;
+    if (!c->prof_on) return;
+    size_t k = c->ev_used[cls];
+    while (c->ev[cls].size() < k + 2) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return;
+      c->ev[cls].push_back(e);
+    }
+    cudaEventRecord(c->ev[cls][k], s);
+    e1 = c->ev[cls][k + 1];
+    c->ev_used[cls] = k + 2;
+  }
+  ~Prof() {
+    if (e1) cudaEventRecord(e1, s);
+  }
+};
+}  // namespace
 
 namespace {
 
@@ -71,6 +103,8 @@ const char *stx_strerror(int code) {
 int stx_ctx_destroy(stx_ctx *c) {
   if (!c) return STX_E_INVALID;
   for (void *p : c->allocs) cudaFree(p);
+  for (int k = 0; k < STX_NK; k++)
+    for (cudaEvent_t e : c->ev[k]) cudaEventDestroy(e);
   delete c;
   return STX_OK;
 }
@@ -221,11 +255,13 @@ int stx_eval_aux(stx_ctx *c, void *s, double *w, double *wa, int i0, int i1, int
   const DevGrid &g = c->d.g;
   if (i0 < 1 - g.ng || i1 > g.nx + g.ng || j0 < 1 - g.ng || j1 > g.ny + g.ng || k0 < 1 - g.ng || k1 > g.nz + g.ng)
     return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_EVAL_AUX, 1);
   return launch_eval_aux(c->d, S(s), w, wa, i0, i1, j0, j1, k0, k1);
 }
 
 int stx_eval_aux2(stx_ctx *c, void *s, double *wa) {
   if (!c || !wa) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_DUCROS, 1);
   return launch_eval_aux2(c->d, S(s), wa);
 }
 
@@ -251,11 +287,13 @@ int stx_compute_aux(stx_ctx *c, void *s, double *w, double *wa, int central, int
 
 int stx_bcextr_var(stx_ctx *c, void *s, double *v) {
   if (!c || !v) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_GHOST, 1);
   return launch_bcextr_var(c->d, S(s), v);
 }
 
 int stx_bcswap(stx_ctx *c, void *s, double *f, int nvar) {
   if (!c || !f || nvar < 1) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_GHOST, (c->periodic[0] || c->periodic[1] || c->periodic[2]) ? 1 : 0);
   return launch_bcswap(c->d, S(s), f, nvar, c->periodic);
 }
 
@@ -263,7 +301,10 @@ int stx_update_ghost(stx_ctx *c, void *s, double *w, int do_swap) {
   if (!c || !w) return STX_E_INVALID;
   for (int ilat = 1; ilat <= 6; ilat++) {
     int tag = c->par.bctags[ilat - 1];
-    if (tag == 1 || tag == 2 || tag == 8) TRY(launch_bc_face(c->d, S(s), w, ilat, tag, c->winf_d));
+    if (tag == 1 || tag == 2 || tag == 8) {
+      Prof pf(c, S(s), STX_K_GHOST, 1);
+      TRY(launch_bc_face(c->d, S(s), w, ilat, tag, c->winf_d));
+    }
   }
   if (do_swap == 1) TRY(stx_bcswap(c, s, w, c->nv));
   return STX_OK;
@@ -272,20 +313,24 @@ int stx_update_ghost(stx_ctx *c, void *s, double *w, int do_swap) {
 // ------------------------------------------------------------------ fluxes
 int stx_euler_x(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nx) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_EULER, 1);
   return launch_euler(c->d, S(s), 0, wa, fl, a, b, ow);
 }
 int stx_euler_y(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.ny) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_EULER, 1);
   return launch_euler(c->d, S(s), 1, wa, fl, a, b, ow);
 }
 int stx_euler_z(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nz) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_EULER, 1);
   return launch_euler(c->d, S(s), 2, wa, fl, a, b, ow);
 }
 
 int stx_visflx(stx_ctx *c, void *s, const double *wa, double *fl, int mode) {
   if (!c || !wa || !fl) return STX_E_INVALID;
   const DevGrid &g = c->d.g;
+  Prof pf(c, S(s), STX_K_VISC, mode == 1 ? (g.nx > 1) + (g.ny > 1) + (g.nz > 1) : 1);
   if (mode == 1) {
     if (g.nx > 1) TRY(launch_visflx(c->d, S(s), 0, wa, fl));
     if (g.ny > 1) TRY(launch_visflx(c->d, S(s), 1, wa, fl));
@@ -299,37 +344,47 @@ int stx_visflx(stx_ctx *c, void *s, const double *wa, double *fl, int mode) {
 // ------------------------------------------------------------------ RK
 int stx_init_flux(stx_ctx *c, void *s, double *fl, double *fln, double rhodt) {
   if (!c || !fl || !fln) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_RK, 1);
   return launch_init_flux(c->d, S(s), fl, fln, nullptr, rhodt);
 }
 int stx_init_flux_simpler(stx_ctx *c, void *s, double *fl, double *fln, const double *fl_sav, double rhodt) {
   if (!c || !fl || !fln || !fl_sav) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_RK, 1);
   return launch_init_flux(c->d, S(s), fl, fln, fl_sav, rhodt);
 }
 int stx_sav_flx(stx_ctx *c, void *s, const double *fl, double *fl_sav) {
   if (!c || !fl || !fl_sav) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_RK, 1);
   return launch_copy(c->d, S(s), fl, fl_sav);
 }
 int stx_update_flux(stx_ctx *c, void *s, const double *fl, double *fln, double gamdt) {
   if (!c || !fl || !fln) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_RK, 1);
   return launch_update_flux(c->d, S(s), fl, fln, nullptr, gamdt);
 }
 int stx_update_simpler_flux(stx_ctx *c, void *s, const double *fl, double *fln, const double *fl_sav, double gamdt) {
   if (!c || !fl || !fln || !fl_sav) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_RK, 1);
   return launch_update_flux(c->d, S(s), fl, fln, fl_sav, gamdt);
 }
 int stx_update_field(stx_ctx *c, void *s, double *w, const double *fln, const int32_t *mask) {
   if (!c || !w || !fln) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_RK, 1);
   return launch_update_field(c->d, S(s), w, nullptr, (double *)fln, nullptr, mask, 0.0, 0);
 }
 int stx_rk_finish(stx_ctx *c, void *s, double *w, const double *fl, double *fln, const double *fl_sav,
                   const int32_t *mask, double gamdt, int simpler) {
   if (!c || !w || !fl || !fln || (simpler == 1 && !fl_sav)) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_RK, 1);
   return launch_update_field(c->d, S(s), w, fl, fln, simpler == 1 ? fl_sav : nullptr, mask, gamdt, 1);
 }
 
 int stx_compute_dt(stx_ctx *c, void *s, const double *wa, const int32_t *mask, double out9[9]) {
   if (!c || !wa || !out9) return STX_E_INVALID;
-  TRY(launch_compute_dt(c->d, S(s), wa, mask, c->dt_d));
+  {
+    Prof pf(c, S(s), STX_K_DT, 1);
+    TRY(launch_compute_dt(c->d, S(s), wa, mask, c->dt_d));
+  }
   unsigned long long h[9];
   STX_CUDA_TRY(cudaMemcpyAsync(h, c->dt_d, sizeof(h), cudaMemcpyDeviceToHost, S(s)));
   STX_CUDA_TRY(cudaStreamSynchronize(S(s)));
@@ -345,17 +400,20 @@ int stx_compute_dt(stx_ctx *c, void *s, const double *wa, const int32_t *mask, d
 int stx_rosenbrock(stx_ctx *c, void *s, double *w, double *wa, double dttry, double t0, double t1) {
   if (!c || !w || !wa) return STX_E_INVALID;
   if (c->d.t.nr < 1) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_CHEM, 1);
   return launch_rosenbrock(c->d, S(s), w, wa, dttry, t0, t1, c->counter_d);
 }
 int stx_rosenbrock_krylov(stx_ctx *c, void *s, double *w, const double *wa, const double *fl_sav, double dttry,
                           double t0, double t1, int simpler) {
   if (!c || !w || !wa || (simpler == 1 && !fl_sav)) return STX_E_INVALID;
   if (c->d.t.nr < 1) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_CHEM, 1);
   return launch_rok4(c->d, S(s), w, wa, fl_sav, dttry, t0, t1, simpler, c->counter_d);
 }
 int stx_compute_chemistry(stx_ctx *c, void *s, double *w, double *wa, double *fl) {
   if (!c || !w || !wa || !fl) return STX_E_INVALID;
   if (c->d.t.nr < 1) return STX_E_INVALID;
+  Prof pf(c, S(s), STX_K_CHEM, 1);
   return launch_chem_explicit(c->d, S(s), w, wa, fl);
 }
 
@@ -370,9 +428,9 @@ static int rhs_pass(stx_ctx *c, void *s, const stx_fields *f) {
   TRY(stx_bcextr_var(c, s, div));
   TRY(stx_bcswap(c, s, duc, 1));
   TRY(stx_bcswap(c, s, div, 1));
-  TRY(launch_euler(c->d, S(s), 0, f->w_aux, f->fl, c->par.eul_imin, c->par.eul_imax, 0));
-  if (g.ny > 1) TRY(launch_euler(c->d, S(s), 1, f->w_aux, f->fl, c->par.eul_jmin, c->par.eul_jmax, 0));
-  if (g.nz > 1) TRY(launch_euler(c->d, S(s), 2, f->w_aux, f->fl, c->par.eul_kmin, c->par.eul_kmax, 0));
+  TRY(stx_euler_x(c, s, f->w_aux, f->fl, c->par.eul_imin, c->par.eul_imax, 0));
+  if (g.ny > 1) TRY(stx_euler_y(c, s, f->w_aux, f->fl, c->par.eul_jmin, c->par.eul_jmax, 0));
+  if (g.nz > 1) TRY(stx_euler_z(c, s, f->w_aux, f->fl, c->par.eul_kmin, c->par.eul_kmax, 0));
   TRY(stx_visflx(c, s, f->w_aux, f->fl, 1));
   TRY(stx_visflx(c, s, f->w_aux, f->fl, 2));
   if (c->par.enable_chemistry == 1) TRY(stx_compute_chemistry(c, s, f->w, f->w_aux, f->fl));
@@ -384,7 +442,8 @@ int stx_rk_sync(stx_ctx *c, void *s, const stx_fields *f, double dt, int simpler
   for (int istep = 0; istep < c->par.nrk; istep++) {
     double rhodt = c->par.rhork[istep] * dt;
     double gamdt = c->par.gamrk[istep] * dt;
-    TRY(launch_init_flux(c->d, S(s), f->fl, f->fln, simpler == 1 ? f->fl_sav : nullptr, rhodt));
+    if (simpler == 1) TRY(stx_init_flux_simpler(c, s, f->fl, f->fln, f->fl_sav, rhodt));
+    else TRY(stx_init_flux(c, s, f->fl, f->fln, rhodt));
     TRY(rhs_pass(c, s, f));
     TRY(stx_rk_finish(c, s, f->w, f->fl, f->fln, f->fl_sav, f->fluid_mask, gamdt, simpler));
     TRY(stx_update_ghost(c, s, f->w, 0));
@@ -418,6 +477,32 @@ int stx_advance_solution(stx_ctx *c, void *s, const stx_fields *f, double dt, do
     }
   } else {
     TRY(stx_rk_sync(c, s, f, dt, 0));
+  }
+  return STX_OK;
+}
+
+int stx_profile_enable(stx_ctx *c, int on) {
+  if (!c) return STX_E_INVALID;
+  c->prof_on = on ? 1 : 0;
+  for (int k = 0; k < STX_NK; k++) {
+    c->launches[k] = 0;
+    c->ev_used[k] = 0;
+  }
+  return STX_OK;
+}
+
+int stx_profile_read(stx_ctx *c, stx_kprof *out) {
+  if (!c || !out) return STX_E_INVALID;
+  STX_CUDA_TRY(cudaDeviceSynchronize());
+  for (int k = 0; k < STX_NK; k++) {
+    out[k].launches = c->launches[k];
+    out[k].timed = (int64_t)(c->ev_used[k] / 2);
+    double ms = 0.0;
+    for (size_t q = 0; q + 1 < c->ev_used[k]; q += 2) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, c->ev[k][q], c->ev[k][q + 1]) == cudaSuccess) ms += t;
+    }
+    out[k].ms = ms;
   }
   return STX_OK;
 }

@@ -28,7 +28,10 @@ class Solver:
             raise RuntimeError("the stx solver needs a CUDA device (there is no CPU fallback)")
         self.lib = load_stx()
         self.case = case
-        self.device = torch.device(device)
+        dev = torch.device(device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
         torch.cuda.set_device(self.device)
         self._par, self._tab, self._grid = case.params_struct(), case.tables_struct(), case.grid_struct()
         ctx = C.c_void_p()
