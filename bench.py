@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the multi-species reacting step (cell-steps/s).
+
+Workload: 3-D periodic reacting decaying turbulence on 256^3 cells per GPU,
+9-species H2/air (phi = 0.7, 1000 K, 1 atm), hybrid WENO5-Z / KEEP(2) fluxes with
+the Ducros sensor, mixture-averaged transport, Strang-split ROK4 chemistry,
+Wray RK3, CFL 0.5, FP64 throughout (the reference method).  One step is the
+reference's integration-loop iteration: CFL reduction, advance_solution
+(Rosenbrock half step, three RK substeps, Rosenbrock half step) and the final
+compute_aux.
+
+  python bench.py [--gpus N --steps K --warmup W]     # this implementation
+  python bench.py --impl reference [...]              # the CPU reference arm
+
+Multi-GPU (torchrun, one rank per GPU): every rank advances its own 256^3 box
+(weak scaling); the CFL maxima are max-reduced over ranks each step, as the
+reference's mpi_allreduce does.  Ghost exchange between ranks is not part of
+this benchmark (each box is periodic on its own).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "prop-streams2_b200"))
+
+METRIC = "cell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="stx", choices=["stx", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="cells per direction per GPU")
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--cpu-n", type=int, default=32, help="box edge of the CPU sample")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the baseline")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer leg (default: --steps)")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def config_dict(n, world, extra=None):
+    d = {"workload": f"3-D periodic reacting decaying turbulence, {n}^3 cells per GPU, 9-species H2/air "
+                     f"(21 reactions), phi=0.7, T=1000 K, p=1 atm, u_rms=0.3 c0, E(k)~k^4 exp(-2(k/4)^2); "
+                     f"hybrid WENO5-Z/KEEP(2) + Ducros (threshold 0.1), mixture-averaged transport, "
+                     f"Strang ROK4, Wray RK3, CFL 0.5",
+         "cells_per_gpu": n ** 3, "species": 9, "reactions": 21, "precision_form": "plain FP64",
+         "parallelism": f"dp{world} (independent periodic boxes, global dt)",
+         "l2": "inputs larger than L2 (about 15 GB of fields per GPU)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.fn = None
+
+    def start(self):
+        try:
+            fd, self.fn = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.fn, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.fn) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax.append(float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.fn)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU (oracle) leg
+def cpu_run(n, steps_budget_s, seed, warm=1, threads=None):
+    """The CPU restatement (oracle) on an n^3 same-resolution sample of the workload:
+    returns (cell-steps/s, cores, sample text)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from stx import configs
+    from driver import OracleSolver
+    threads = threads or os.cpu_count() or 1
+    c = configs.turbulence_case(n, alloc_fields=True)
+    W, WA = configs.turbulence_fields(c, seed)
+    c.w[...] = W
+    c.w_aux[...] = WA
+    o = OracleSolver(c, threads=threads)
+    o.prepare()
+    for _ in range(warm):
+        o.step()
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        o.step()
+        k += 1
+        el = time.perf_counter() - t0
+        if el >= steps_budget_s or k >= 1000:
+            break
+    o.close()
+    rate = n ** 3 * k / el
+    return rate, threads, f"{n}^3 cells (same grid spacing and state statistics), {k} steps after {warm} warm-up, {el:.1f} s"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    oracle_so = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.exists(oracle_so):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    # W warm-up steps, then K timed steps of the CPU implementation on a bounded sample
+    budget = max(5.0, min(60.0, 6.0 * args.steps))
+    rate, cores, sample = cpu_run(args.cpu_n, budget, args.seed, warm=max(1, min(args.warmup, 2)))
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": config_dict(args.n, args.gpus, {"reference_impl": "CPU restatement of the reference's FP64 "
+                                                      "kernels (oracle/, OpenMP), not the reference binary: the "
+                                                      "CUDA-Fortran reference cannot be compiled here"}),
+            "cpu_baseline": {"value": rate, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU leg
+KNAMES = ["eval_aux", "ducros", "ghost", "euler", "visc", "rk", "chem", "dt"]
+
+
+def run_stx(args):
+    import ctypes as C
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from stx import configs
+    from stx.native import check
+    from stx.solver import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    n = args.n
+    case = configs.turbulence_case(n)
+    W, WA = configs.turbulence_fields(case, args.seed + rank, xp=torch, device=dev)
+    sol = Solver(case, device=str(dev), w=W, w_aux=WA)
+    del W, WA
+    lib = sol.lib
+
+    def compute_dt_global():
+        out = (C.c_double * 9)()
+        check(lib.stx_compute_dt(sol.ctx, sol.stream, C.c_void_p(sol.w_aux.data_ptr()), None, out), "compute_dt")
+        m = torch.tensor(list(out), dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        sol.dt = case.cfl / float(m.max())
+        return sol.dt
+
+    def step():
+        sol.icyc += 1
+        sol.compute_aux(1, 0)
+        compute_dt_global()
+        sol.advance_solution()
+        sol.compute_aux(1, 0)
+        sol.time += sol.dt
+
+    sol.update_ghost(1)
+    sol.compute_aux(1, 1)
+    check(lib.stx_bcextr_var(sol.ctx, sol.stream, sol.aux_slot(case.J("DIV"))), "bcextr")
+    check(lib.stx_bcswap(sol.ctx, sol.stream, sol.aux_slot(case.J("DIV")), 1), "bcswap")
+    check(lib.stx_bcswap(sol.ctx, sol.stream, sol.aux_slot(case.J("DUC")), 1), "bcswap")
+    sol.fl.zero_()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---------------- timed region: device-resident fields
+    from stx.native import StxKprof  # noqa: F401  (declared below if absent)
+    check(lib.stx_profile_enable(sol.ctx, 1), "profile")
+    clocks = Clocks(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    prof = (StxKprof * 8)()
+    check(lib.stx_profile_read(sol.ctx, prof), "profile_read")
+    check(lib.stx_profile_enable(sol.ctx, 0), "profile")
+    ms_all = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms_all, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_all.item())
+    value = (n ** 3) * world * args.steps / (ms_max / 1e3)
+    launches = int(sum(p.launches for p in prof))
+    status = sol.status()
+
+    # ---------------- e2e: the same step through the C ABI with host buffers
+    K2 = args.e2e_steps or args.steps
+    host_w = torch.empty(sol.w.shape, dtype=torch.float64, pin_memory=True)
+    host_w.copy_(sol.w)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(K2):
+        sol.w.copy_(host_w, non_blocking=True)
+        step()
+        host_w.copy_(sol.w, non_blocking=True)
+    t1.record()
+    torch.cuda.synchronize()
+    ms2 = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms2, op=dist.ReduceOp.MAX)
+    e2e_value = (n ** 3) * world * K2 / (float(ms2.item()) / 1e3)
+    wbytes = sol.w.numel() * 8
+
+    # ---------------- roofline of the dominant HBM-bound kernel class
+    cls = {KNAMES[k]: {"launches": int(prof[k].launches), "ms": prof[k].ms, "bytes": prof[k].bytes}
+           for k in range(8)}
+    tot_ms = sum(v["ms"] for v in cls.values()) or 1.0
+    for v in cls.values():
+        v["share"] = v["ms"] / tot_ms
+        v["gbs"] = (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] > 0 and v["bytes"] > 0 else None
+    hbm_classes = [k for k in cls if k != "chem" and cls[k]["bytes"] > 0]
+    dom = max(hbm_classes, key=lambda k: cls[k]["ms"])
+    peaks_fn = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback 6.65 TB/s"
+    if os.path.exists(peaks_fn):
+        with open(peaks_fn) as fh:
+            peak = float(json.load(fh)["hbm_gbs"])
+        peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+    traffic = None
+    tfn = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tfn):
+        with open(tfn) as fh:
+            tr = json.load(fh)
+        traffic = tr.get(dom, {}).get("dram_bytes_per_launch")
+    ach = cls[dom]["gbs"]
+    roofline = {"bound": "hbm", "kernel_class": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak if ach else None, "traffic": traffic, "peak_source": peak_src,
+                "launches": cls[dom]["launches"],
+                "bytes_per_launch": cls[dom]["bytes"] / max(1, cls[dom]["launches"])}
+
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": config_dict(n, world, {"dt_last": sol.dt}),
+            "roofline": roofline, "clocks": ck, "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": wbytes, "d2h_bytes_per_step": wbytes,
+                    "path": "stx_advance_solution et al. through the C ABI, state w copied from pinned host memory "
+                            "before and back after every step"},
+            "kernels": cls, "status_bits": status}
+    if world == 1 and rank == 0 and not args.no_cpu:
+        rate, cores, sample = cpu_run(args.cpu_n, args.cpu_budget, args.seed)
+        line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_stx(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -198,6 +198,8 @@ typedef struct stx_kprof {
   int64_t launches;    /* kernel launches since the last stx_profile_enable */
   int64_t timed;       /* entry-point calls timed with events */
   double  ms;          /* summed event time of the timed calls */
+  double  bytes;       /* algorithmic HBM bytes of those calls: every field the
+                          kernel must read or write, once (FP64) */
 } stx_kprof;
 /* Reset the counters; on != 0 also records events around every launch. */
 int stx_profile_enable(stx_ctx *ctx, int on);

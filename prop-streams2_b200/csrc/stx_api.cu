@@ -25,7 +25,12 @@ struct stx_ctx {
   long long launches[STX_NK];
   std::vector<cudaEvent_t> ev[STX_NK];   // begin/end pairs
   size_t ev_used[STX_NK];
+  double bytes[STX_NK];                  // algorithmic bytes of the timed calls
 };
+
+// algorithmic FP64 bytes per point of each kernel (every field it must read or
+// write, once): ns species, nv = ns + 4
+static inline double B8(double n) { return 8.0 * n; }
 
 namespace {
 // Counts the kernels an entry point launches and, with profiling on, brackets
@@ -35,9 +40,10 @@ struct Prof {
   cudaStream_t s;
   int cls;
   cudaEvent_t e1 = nullptr;
-  Prof(stx_ctx *c_, cudaStream_t s_, int cls_, int nlaunch) : c(c_), s(s_), cls(cls_) {
+  Prof(stx_ctx *c_, cudaStream_t s_, int cls_, int nlaunch, double bytes = 0.0) : c(c_), s(s_), cls(cls_) {
     c->launches[cls] += nlaunch;
     if (!c->prof_on) return;
+    c->bytes[cls] += bytes;
     size_t k = c->ev_used[cls];
     while (c->ev[cls].size() < k + 2) {
       cudaEvent_t e;
@@ -255,13 +261,15 @@ int stx_eval_aux(stx_ctx *c, void *s, double *w, double *wa, int i0, int i1, int
   const DevGrid &g = c->d.g;
   if (i0 < 1 - g.ng || i1 > g.nx + g.ng || j0 < 1 - g.ng || j1 > g.ny + g.ng || k0 < 1 - g.ng || k1 > g.nz + g.ng)
     return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_EVAL_AUX, 1);
+  // reads w (nv) and the T guess; writes Y, u, v, w, h, T, p, c, rho, Z, mu, lambda, rho*D
+  Prof pf(c, S(s), STX_K_EVAL_AUX, 1,
+          (double)(i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1) * B8(3 * c->ns + 16));
   return launch_eval_aux(c->d, S(s), w, wa, i0, i1, j0, j1, k0, k1);
 }
 
 int stx_eval_aux2(stx_ctx *c, void *s, double *wa) {
   if (!c || !wa) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_DUCROS, 1);
+  Prof pf(c, S(s), STX_K_DUCROS, 1, (double)c->d.g.npi * B8(5));
   return launch_eval_aux2(c->d, S(s), wa);
 }
 
@@ -313,24 +321,29 @@ int stx_update_ghost(stx_ctx *c, void *s, double *w, int do_swap) {
 // ------------------------------------------------------------------ fluxes
 int stx_euler_x(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nx) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_EULER, 1);
+  // reads Y, rho, u, v, w, h, p, c, Ducros (ns+8) and fl (unless overwritten); writes fl
+  Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.ny * c->d.g.nz * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
   return launch_euler(c->d, S(s), 0, wa, fl, a, b, ow);
 }
 int stx_euler_y(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.ny) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_EULER, 1);
+  Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.nx * c->d.g.nz * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
   return launch_euler(c->d, S(s), 1, wa, fl, a, b, ow);
 }
 int stx_euler_z(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nz) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_EULER, 1);
+  Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.nx * c->d.g.ny * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
   return launch_euler(c->d, S(s), 2, wa, fl, a, b, ow);
 }
 
 int stx_visflx(stx_ctx *c, void *s, const double *wa, double *fl, int mode) {
   if (!c || !wa || !fl) return STX_E_INVALID;
   const DevGrid &g = c->d.g;
-  Prof pf(c, S(s), STX_K_VISC, mode == 1 ? (g.nx > 1) + (g.ny > 1) + (g.nz > 1) : 1);
+  const int ndir = (g.nx > 1) + (g.ny > 1) + (g.nz > 1);
+  // mode 1, per direction: u, v, w, T, mu, lambda, Y, rho*D read and fl read+written;
+  // mode 2: u, v, w, mu, div read and four fl components read+written
+  Prof pf(c, S(s), STX_K_VISC, mode == 1 ? ndir : 1,
+          mode == 1 ? (double)g.npi * ndir * B8(4 * c->ns + 14) : (double)g.npi * B8(13));
   if (mode == 1) {
     if (g.nx > 1) TRY(launch_visflx(c->d, S(s), 0, wa, fl));
     if (g.ny > 1) TRY(launch_visflx(c->d, S(s), 1, wa, fl));
@@ -344,7 +357,7 @@ int stx_visflx(stx_ctx *c, void *s, const double *wa, double *fl, int mode) {
 // ------------------------------------------------------------------ RK
 int stx_init_flux(stx_ctx *c, void *s, double *fl, double *fln, double rhodt) {
   if (!c || !fl || !fln) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_RK, 1);
+  Prof pf(c, S(s), STX_K_RK, 1, (double)c->d.g.npi * B8(3 * c->nv));
   return launch_init_flux(c->d, S(s), fl, fln, nullptr, rhodt);
 }
 int stx_init_flux_simpler(stx_ctx *c, void *s, double *fl, double *fln, const double *fl_sav, double rhodt) {
@@ -375,14 +388,14 @@ int stx_update_field(stx_ctx *c, void *s, double *w, const double *fln, const in
 int stx_rk_finish(stx_ctx *c, void *s, double *w, const double *fl, double *fln, const double *fl_sav,
                   const int32_t *mask, double gamdt, int simpler) {
   if (!c || !w || !fl || !fln || (simpler == 1 && !fl_sav)) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_RK, 1);
+  Prof pf(c, S(s), STX_K_RK, 1, (double)c->d.g.npi * B8((simpler == 1 ? 6 : 5) * c->nv));
   return launch_update_field(c->d, S(s), w, fl, fln, simpler == 1 ? fl_sav : nullptr, mask, gamdt, 1);
 }
 
 int stx_compute_dt(stx_ctx *c, void *s, const double *wa, const int32_t *mask, double out9[9]) {
   if (!c || !wa || !out9) return STX_E_INVALID;
   {
-    Prof pf(c, S(s), STX_K_DT, 1);
+    Prof pf(c, S(s), STX_K_DT, 1, (double)c->d.g.npi * B8(c->ns + 8));
     TRY(launch_compute_dt(c->d, S(s), wa, mask, c->dt_d));
   }
   unsigned long long h[9];
@@ -407,7 +420,7 @@ int stx_rosenbrock_krylov(stx_ctx *c, void *s, double *w, const double *wa, cons
                           double t0, double t1, int simpler) {
   if (!c || !w || !wa || (simpler == 1 && !fl_sav)) return STX_E_INVALID;
   if (c->d.t.nr < 1) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_CHEM, 1);
+  Prof pf(c, S(s), STX_K_CHEM, 1, (double)c->d.g.npi * B8(2 * c->nv + 2));
   return launch_rok4(c->d, S(s), w, wa, fl_sav, dttry, t0, t1, simpler, c->counter_d);
 }
 int stx_compute_chemistry(stx_ctx *c, void *s, double *w, double *wa, double *fl) {
@@ -487,6 +500,7 @@ int stx_profile_enable(stx_ctx *c, int on) {
   for (int k = 0; k < STX_NK; k++) {
     c->launches[k] = 0;
     c->ev_used[k] = 0;
+    c->bytes[k] = 0.0;
   }
   return STX_OK;
 }
@@ -503,6 +517,7 @@ int stx_profile_read(stx_ctx *c, stx_kprof *out) {
       if (cudaEventElapsedTime(&t, c->ev[k][q], c->ev[k][q + 1]) == cudaSuccess) ms += t;
     }
     out[k].ms = ms;
+    out[k].bytes = c->bytes[k];
   }
   return STX_OK;
 }

@@ -79,7 +79,7 @@ class Config:
 class Case:
     """Everything the kernels need for one solve, on the host."""
 
-    def __init__(self, cfg: Config, tables: M.Tables, init_Y: Optional[np.ndarray] = None):
+    def __init__(self, cfg: Config, tables: M.Tables, init_Y: Optional[np.ndarray] = None, alloc_fields: bool = True):
         self.cfg = cfg
         self.tb = tables
         ns = tables.ns
@@ -180,6 +180,11 @@ class Case:
         self.eul = [1, self.nx, 1, self.ny, 1, self.nz]
         # --- fields
         self.nxg, self.nyg, self.nzg = self.nx + 2 * self.ng, self.ny + 2 * self.ng, self.nz + 2 * self.ng
+        self._keep = []
+        self.fluid_mask = None
+        if not alloc_fields:      # fields are built on the device by the caller
+            self.w = self.w_aux = None
+            return
         self.w = np.empty((self.nv, self.nzg, self.nyg, self.nxg))
         for m in range(self.nv):
             self.w[m] = self.winf[m]

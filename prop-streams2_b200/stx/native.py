@@ -68,6 +68,10 @@ class StxFields(C.Structure):
                 ("fl_sav", C.c_void_p), ("fluid_mask", C.c_void_p)]
 
 
+class StxKprof(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("timed", C.c_int64), ("ms", C.c_double), ("bytes", C.c_double)]
+
+
 _VP = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -102,6 +106,8 @@ STX_SIGNATURES = [
     ("stx_rk_sync", _I, [_VP, _VP, C.POINTER(StxFields), _D, _I]),
     ("stx_advance_solution", _I, [_VP, _VP, C.POINTER(StxFields), _D, _D]),
     ("stx_status", _I, [_VP, _VP, C.POINTER(C.c_uint32), _I]),
+    ("stx_profile_enable", _I, [_VP, _I]),
+    ("stx_profile_read", _I, [_VP, C.POINTER(StxKprof)]),
 ]
 
 ORACLE_SIGNATURES = [

@@ -23,7 +23,8 @@ def _p(t: Optional[torch.Tensor]):
 
 
 class Solver:
-    def __init__(self, case, device: str = "cuda"):
+    def __init__(self, case, device: str = "cuda", w: Optional[torch.Tensor] = None,
+                 w_aux: Optional[torch.Tensor] = None):
         if not torch.cuda.is_available():
             raise RuntimeError("the stx solver needs a CUDA device (there is no CPU fallback)")
         self.lib = load_stx()
@@ -39,8 +40,14 @@ class Solver:
               "stx_ctx_create")
         self.ctx = ctx
         nv = case.nv
-        self.w = torch.from_numpy(case.w).to(self.device).contiguous()
-        self.w_aux = torch.from_numpy(case.w_aux).to(self.device).contiguous()
+        if w is None:
+            w = torch.from_numpy(case.w).to(self.device)
+        if w_aux is None:
+            w_aux = torch.from_numpy(case.w_aux).to(self.device)
+        self.w = w.contiguous()
+        self.w_aux = w_aux.contiguous()
+        assert self.w.shape == (nv, case.nzg, case.nyg, case.nxg) and self.w.dtype == torch.float64
+        assert self.w_aux.shape == (case.nv_aux, case.nzg, case.nyg, case.nxg)
         shp = (nv, case.nz, case.ny, case.nx)
         self.fl = torch.zeros(shp, dtype=torch.float64, device=self.device)
         self.fln = torch.zeros(shp, dtype=torch.float64, device=self.device)
