@@ -141,6 +141,11 @@ def turbulence_fields(c, seed: int, xp=np, device=None):
         import torch
         W = torch.zeros(shape, dtype=torch.float64, device=device)
         WA = torch.zeros((c.nv_aux, c.nzg, c.nyg, c.nxg), dtype=torch.float64, device=device)
+    # every point, ghost edges and corners included, starts from the mean state
+    # (initial_conditions, multideal.F90:3703-3705), then the interior is set
+    for k in range(ns):
+        W[k] = rho * Y[k]
+    W[ns + 3] = rho * e0
     sl = (slice(ng, ng + n),) * 3
     for k in range(ns):
         W[(k,) + sl] = rho * Y[k]
