@@ -11,375 +11,7 @@
 // operations as the reference, so the result is independent of the schedule.
 // This file is compiled without FMA contraction so that its arithmetic matches
 // the FP64 oracle operation by operation (libm vs CUDA exp/pow/log10 aside).
-#include "stx_kernels.cuh"
-
-// Production terms of rosenbrock_rhs / rosenbrock_krylov_rhs / compute_chemistry_cuf
-// (kernels_gpu.F90:9251-9357): rhs_k += W_k sum_r (nu''_kr - nu'_kr) q_r, summed
-// over reactions in order for every species.  explicit_form selects the explicit
-// kernel's form (every species term, :9654-9661) instead of the Rosenbrock one.
-template <int NS>
-__device__ void chem_source(const DevTab &t, double tt, const double *conc, double *rhs, bool explicit_form) {
-  const int nr = t.nr;
-  double Rtti = 1.0 / (t.Ru * tt);
-  int itt;
-  double dtt;
-  {
-    itt = (int)((tt - t.tmin) / t.dtab) + 1;
-    if (itt < 1) itt = 1;
-    if (itt > t.ntab) itt = t.ntab;
-    double ttleft = (itt - 1) * t.dtab + t.tmin;
-    dtt = (tt - ttleft) / t.dtab;
-  }
-  const double *kcrow = t.kc_r + (long long)(itt - 1) * nr;
-#pragma unroll 1
-  for (int lr = 0; lr < nr; lr++) {
-    int ty = __ldg(t.reac_ty + lr);
-    double kf, k0, kinf, tb, rpres;
-    double A1 = ldg(t.arr_a + lr), B1 = ldg(t.arr_b + lr), E1 = ldg(t.arr_ea + lr);
-    if (ty == 0 || ty == 1) {
-      kf = A1;
-      if (B1 != 0.0) kf = kf * pow(tt, B1);
-      if (E1 != 0.0) kf = kf * exp(-E1 * Rtti);
-    } else {
-      double A2 = ldg(t.arr_a + nr + lr), B2 = ldg(t.arr_b + nr + lr), E2 = ldg(t.arr_ea + nr + lr);
-      k0 = A1 * pow(tt, B1) * exp(-E1 * Rtti);
-      kinf = A2 * pow(tt, B2) * exp(-E2 * Rtti);
-      tb = 0.0;
-#pragma unroll
-      for (int k = 0; k < NS; k++) tb = tb + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k];
-      rpres = k0 * tb / kinf;
-      if (ty == 2) {
-        kf = kinf * (rpres / (1.0 + rpres));
-      } else if (ty == 3) {
-        if (rpres < 1e-30) {
-          kf = k0 * tb;
-        } else {
-          double F1 = ldg(t.falloff + lr), F2 = ldg(t.falloff + nr + lr), F3 = ldg(t.falloff + 2 * nr + lr),
-                 F4 = ldg(t.falloff + 3 * nr + lr);
-          double fcent = (1.0 - F1) * exp(-tt / F2) + F1 * exp(-tt / F3);
-          if (F4 != -3.14) fcent = fcent + exp(-F4 / tt);
-          fcent = log10(fcent);
-          double coff = -0.4 - 0.67 * fcent;
-          double noff = 0.75 - 1.27 * fcent;
-          double doff = 0.14;
-          double lp = log10(rpres);
-          double foff = pow(10.0, pow(1.0 + pow((lp + coff) / (noff - doff * (lp + coff)), 2.0), -1.0) * fcent);
-          kf = kinf * (rpres / (1.0 + rpres)) * foff;
-        }
-      } else if (ty == 4) {
-        double F1 = ldg(t.falloff + lr), F2 = ldg(t.falloff + nr + lr), F3 = ldg(t.falloff + 2 * nr + lr),
-               F4 = ldg(t.falloff + 3 * nr + lr), F5 = ldg(t.falloff + 4 * nr + lr);
-        double xoff = 1.0 / (1.0 + pow(log10(rpres), 2.0));
-        double foff = F4 * pow(F1 * exp(-F2 / tt) + exp(-tt / F3), xoff) * pow(tt, F5);
-        kf = kinf * (rpres / (1.0 + rpres)) * foff;
-      } else {
-        kf = 0.0;
-      }
-    }
-    double kb;
-    if (__ldg(t.is_rev + lr) == 1) {
-      double a = ldg(kcrow + lr);
-      double dkc = ldg(kcrow + nr + lr) - a;
-      double kc = a + dkc * dtt;
-      kb = kf / kc;
-    } else {
-      kb = 0.0;
-    }
-    double q1 = 1.0, q2 = 1.0;
-#pragma unroll
-    for (int k = 0; k < NS; k++) {
-      double rr = ldg(t.r_coeffs + (long long)k * nr + lr), pp = ldg(t.p_coeffs + (long long)k * nr + lr);
-      if (rr == 1.0) q1 = q1 * conc[k];
-      else if (rr != 0.0) q1 = q1 * pow(conc[k], rr);
-      if (pp == 1.0) q2 = q2 * conc[k];
-      else if (pp != 0.0) q2 = q2 * pow(conc[k], pp);
-    }
-    tb = 1.0;
-    if (ty == 1) {
-      tb = 0.0;
-#pragma unroll
-      for (int k = 0; k < NS; k++) tb = tb + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k];
-    }
-    double qlr = tb * (kf * q1 - kb * q2);
-#pragma unroll
-    for (int k = 0; k < NS; k++) {
-      double rr = ldg(t.r_coeffs + (long long)k * nr + lr), pp = ldg(t.p_coeffs + (long long)k * nr + lr);
-      if (explicit_form) {
-        rhs[k] = rhs[k] - (pp - rr) * qlr * ldg(t.mw + k);
-      } else if (rr != 0.0 || pp != 0.0) {
-        double wdtkj = (pp - rr) * qlr;
-        rhs[k] = rhs[k] + wdtkj * ldg(t.mw + k);
-      }
-    }
-  }
-}
-
-// rosenbrock_krylov_rhs (kernels_gpu.F90:10794-10976), PaSR off
-template <int NS>
-__device__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, double *rhs) {
-  const DevTab &t = c.t;
-  double Y[NS], conc[NS], wl[NS];
-#pragma unroll
-  for (int k = 0; k < NS; k++) wl[k] = w_sav[k] > 0.0 ? w_sav[k] : 0.0;
-  double rho = wl[0];
-#pragma unroll
-  for (int k = 1; k < NS; k++) rho = rho + wl[k];
-  double ri = 1.0 / rho;
-#pragma unroll
-  for (int k = 0; k < NS; k++) {
-    Y[k] = wl[k] * ri;
-    conc[k] = rho * Y[k] / ldg(t.mw + k);
-  }
-  double uu = w_sav[NS] * ri, vv = w_sav[NS + 1] * ri, ww = w_sav[NS + 2] * ri;
-  double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-  double ee = (w_sav[NS + 3] * ri) - qq;
-  double tt = temp_from_e<NS>(t, c.p, ee, T_iter, Y);
-#pragma unroll
-  for (int m = 0; m < NS + 4; m++) rhs[m] = 0.0;
-  chem_source<NS>(t, tt, conc, rhs, false);
-}
-
-template <int NV>
-__device__ __forceinline__ double norm2v(const double *v) {
-  double s = 0.0;
-#pragma unroll
-  for (int q = 0; q < NV; q++) s = s + v[q] * v[q];
-  return sqrt(s);
-}
-
-// inv_matrix_krylov with ludcmp_krylov / lubksb_krylov (kernels_gpu.F90:11061-11205)
-// on the leading d x d block of a column-major 4x4 matrix.
-__device__ void inv_matrix_k(double *a, int d) {
-#define AK(r, s) a[((s) - 1) * STX_MMAX + (r) - 1]
-  if (d == 1) { AK(1, 1) = 1.0 / AK(1, 1); return; }
-  int indx[STX_MMAX] = {1, 2, 3, 4};
-  const double tiny = 1.5e-16;
-  double vv[STX_MMAX];
-  bool early = false;
-  for (int i = 1; i <= d && !early; i++) {
-    double amax = 0.0;
-    for (int j = 1; j <= d; j++) if (fabs(AK(i, j)) > amax) amax = fabs(AK(i, j));
-    if (amax < tiny) early = true;
-    else vv[i - 1] = 1.0 / amax;
-  }
-  if (!early) {
-    for (int j = 1; j <= d; j++) {
-      for (int i = 1; i <= j - 1; i++) {
-        double summ = AK(i, j);
-        for (int k = 1; k <= i - 1; k++) summ = summ - AK(i, k) * AK(k, j);
-        AK(i, j) = summ;
-      }
-      double amax = 0.0;
-      int imax = j;
-      for (int i = j; i <= d; i++) {
-        double summ = AK(i, j);
-        for (int k = 1; k <= j - 1; k++) summ = summ - AK(i, k) * AK(k, j);
-        AK(i, j) = summ;
-        double dum = vv[i - 1] * fabs(summ);
-        if (dum >= amax) { imax = i; amax = dum; }
-      }
-      if (j != imax) {
-        for (int k = 1; k <= d; k++) { double dum = AK(imax, k); AK(imax, k) = AK(j, k); AK(j, k) = dum; }
-        vv[imax - 1] = vv[j - 1];
-      }
-      indx[j - 1] = imax;
-      if (fabs(AK(j, j)) < tiny) AK(j, j) = tiny;
-      if (j != d) {
-        double dum = 1.0 / AK(j, j);
-        for (int i = j + 1; i <= d; i++) AK(i, j) = AK(i, j) * dum;
-      }
-    }
-  }
-  double y[STX_MMAX * STX_MMAX];
-  for (int r = 1; r <= d; r++) for (int s = 1; s <= d; s++) y[(s - 1) * STX_MMAX + r - 1] = (r == s) ? 1.0 : 0.0;
-  for (int s = 1; s <= d; s++) {
-    double *b = y + (s - 1) * STX_MMAX;
-    int ii = 0;
-    for (int i = 1; i <= d; i++) {
-      int ll = indx[i - 1];
-      double summ = b[ll - 1];
-      b[ll - 1] = b[i - 1];
-      if (ii != 0) { for (int j = ii; j <= i - 1; j++) summ = summ - AK(i, j) * b[j - 1]; }
-      else if (summ != 0.0) ii = i;
-      b[i - 1] = summ;
-    }
-    for (int i = d; i >= 1; i--) {
-      double summ = b[i - 1];
-      if (i < d) for (int j = i + 1; j <= d; j++) summ = summ - AK(i, j) * b[j - 1];
-      b[i - 1] = summ / AK(i, i);
-    }
-  }
-  for (int r = 1; r <= d; r++) for (int s = 1; s <= d; s++) AK(r, s) = y[(s - 1) * STX_MMAX + r - 1];
-#undef AK
-}
-
-// One ROK4 cell (rosenbrock_krylov_kernel body, :10463-10610).  V holds the
-// Krylov basis; the basis handed back (Vb) is its first mA columns.
-template <int NS>
-__device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const double *fls, double dttry, double time_start,
-                          double time_end, int simpler) {
-  const int NV = NS + 4;
-  const double gam = 0.572816062482135;
-  const double a21 = 0.432364435748567, a31 = -0.514211316876170, a32 = 1.382271144617360;
-  const double a41 = -0.514211316876170, a42 = 1.382271144617360, a43 = 0.0;
-  const double bs1 = 0.194335256262729, bs2 = 0.483167813989227, bs3 = 0.0, bs4 = 0.322496929748044;
-  const double g21 = -0.602765307997356, g31 = -1.389195789724843, g32 = 1.072950969011413;
-  const double g41 = 0.992356412977094, g42 = -1.390032613873701, g43 = -0.440875890223325;
-  const double bt1 = -0.217819895945721, bt2 = 1.03130847478467, bt3 = 0.186511421161047, bt4 = 0.0;
-  const double alpha[4][3] = {{0, 0, 0}, {a21, 0, 0}, {a31, a32, 0}, {a41, a42, a43}};
-  const double gmc[4][3] = {{0, 0, 0}, {g21, 0, 0}, {g31, g32, 0}, {g41, g42, g43}};
-  const double bsv[4] = {bs1, bs2, bs3, bs4}, btv[4] = {bt1, bt2, bt3, bt4};
-  double V[NV * (STX_MMAX + 1)];
-  double inv[STX_MMAX * STX_MMAX];
-  double Am[NV * STX_MMAX];
-  double Ks[NV * STX_NSTAGE];
-  double rhs_sav[NV];
-  int mA = 0;
-#pragma unroll
-  for (int q = 0; q < STX_MMAX * STX_MMAX; q++) inv[q] = 0.0;
-  double time = time_start, dt = dttry, errn = 1.0;
-  int it = 0;
-  while (time < (time_end - 1.0e-12)) {
-    dt = dmin_(dt, time_end - time);
-    it = it + 1;
-    // ---- arnoldi (:10664-10792)
-    {
-      const double TOL = 1e-6, eps = 1.0e-08;
-      double HH[(STX_MMAX + 1) * STX_MMAX], HI[STX_MMAX * STX_MMAX], prj[STX_MMAX], lam[STX_MMAX];
-#pragma unroll
-      for (int q = 0; q < (STX_MMAX + 1) * STX_MMAX; q++) HH[q] = 0.0;
-#pragma unroll
-      for (int q = 0; q < STX_MMAX * STX_MMAX; q++) HI[q] = 0.0;
-#pragma unroll
-      for (int q = 0; q < NV * (STX_MMAX + 1); q++) V[q] = 0.0;
-      mA = 0;
-      krylov_rhs<NS>(c, VEC, T_iter, rhs_sav);
-      if (simpler == 1)
-        for (int m = 0; m < NV; m++) rhs_sav[m] = rhs_sav[m] - fls[m];
-      double nrm = norm2v<NV>(rhs_sav);
-      for (int m = 0; m < NV; m++) V[m] = rhs_sav[m] / nrm;
-      for (int kk = 1; kk <= STX_MMAX; kk++) {
-        double jac[NV], wl[NV];
-        for (int m = 0; m < NV; m++) wl[m] = VEC[m] + (eps * V[(kk - 1) * NV + m]);
-        krylov_rhs<NS>(c, wl, T_iter, jac);
-        if (simpler == 1)
-          for (int m = 0; m < NV; m++) jac[m] = jac[m] - fls[m];
-        for (int m = 0; m < NV; m++) jac[m] = (jac[m] - rhs_sav[m]) / eps;
-        for (int jj = 1; jj <= kk; jj++) {
-          double dot = 0.0;
-          for (int m = 0; m < NV; m++) dot = dot + V[(jj - 1) * NV + m] * jac[m];
-          HH[(kk - 1) * (STX_MMAX + 1) + jj - 1] = dot;
-          for (int m = 0; m < NV; m++) jac[m] = jac[m] - (dot * V[(jj - 1) * NV + m]);
-        }
-        double hn = norm2v<NV>(jac);
-        HH[(kk - 1) * (STX_MMAX + 1) + kk] = hn;
-        for (int m = 0; m < NV; m++) V[kk * NV + m] = jac[m] / hn;
-        // projections of rhs_sav on the first kk basis vectors (the rest are zero)
-        for (int ll = 1; ll <= STX_MMAX; ll++) {
-          double s = 0.0;
-          if (ll <= kk)
-            for (int m = 0; m < NV; m++) s = s + V[(ll - 1) * NV + m] * rhs_sav[m];
-          prj[ll - 1] = s;
-        }
-        for (int n = 1; n <= kk; n++)
-          for (int nn = 1; nn <= kk; nn++) {
-            double h = -(dt * gam * HH[(nn - 1) * (STX_MMAX + 1) + n - 1]);
-            if (n == nn) h = h + 1.0;
-            HI[(nn - 1) * STX_MMAX + n - 1] = h;
-          }
-        for (int n = kk + 1; n <= STX_MMAX; n++) HI[(n - 1) * STX_MMAX + n - 1] = 1.0;
-        inv_matrix_k(HI, kk);
-        for (int ll = 1; ll <= STX_MMAX; ll++) {
-          double s = 0.0;
-          for (int jj = 1; jj <= STX_MMAX; jj++) s = s + HI[(jj - 1) * STX_MMAX + ll - 1] * prj[jj - 1];
-          lam[ll - 1] = s;
-        }
-        if (fabs(dt * gam * hn) * fabs(lam[kk - 1]) < TOL) {
-          mA = kk;
-#pragma unroll
-          for (int q = 0; q < STX_MMAX * STX_MMAX; q++) inv[q] = HI[q];
-          break;
-        }
-      }
-    }
-    // ---- A = Vb (I - inv)  (Vb = first mA columns of V, zero beyond)
-    for (int kk = 1; kk <= STX_MMAX; kk++)
-      for (int ll = 0; ll < NV; ll++) {
-        double idf = ((1 == kk) ? 1.0 : 0.0) - inv[(kk - 1) * STX_MMAX + 0];
-        double a = (mA >= 1 ? V[ll] : 0.0) * idf;
-        for (int jj = 2; jj <= STX_MMAX; jj++) {
-          double vb = (jj <= mA) ? V[(jj - 1) * NV + ll] : 0.0;
-          idf = ((jj == kk) ? 1.0 : 0.0) - inv[(kk - 1) * STX_MMAX + jj - 1];
-          a = a + vb * idf;
-        }
-        Am[(kk - 1) * NV + ll] = a;
-      }
-    // ---- stages; B(ll,jj) = sum_q A(ll,q) Vb(jj,q) is recomputed where used
-    for (int ii = 1; ii <= STX_NSTAGE; ii++) {
-      double ys[NV], F[NV], GK[NV];
-      for (int m = 0; m < NV; m++) ys[m] = VEC[m];
-      for (int jj = 1; jj <= ii - 1; jj++)
-        for (int m = 0; m < NV; m++) ys[m] = ys[m] + dt * alpha[ii - 1][jj - 1] * Ks[(jj - 1) * NV + m];
-      krylov_rhs<NS>(c, ys, T_iter, F);
-      for (int m = 0; m < NV; m++) GK[m] = 0.0;
-      for (int jj = 1; jj <= ii - 1; jj++)
-        for (int m = 0; m < NV; m++) GK[m] = GK[m] + gmc[ii - 1][jj - 1] / gam * Ks[(jj - 1) * NV + m];
-      for (int m = 0; m < NV; m++) F[m] = F[m] + GK[m];
-      if (simpler == 1)
-        for (int m = 0; m < NV; m++) F[m] = F[m] - fls[m];
-      for (int ll = 0; ll < NV; ll++) {
-        double s = 0.0;
-        for (int jj = 0; jj < NV; jj++) {
-          double b = Am[ll] * (mA >= 1 ? V[jj] : 0.0);
-          for (int q = 2; q <= STX_MMAX; q++) b = b + Am[(q - 1) * NV + ll] * ((q <= mA) ? V[(q - 1) * NV + jj] : 0.0);
-          s = (jj == 0) ? b * F[0] : s + b * F[jj];
-        }
-        Ks[(ii - 1) * NV + ll] = F[ll] - s - GK[ll];
-      }
-    }
-    double ys[NV], errv[NV];
-    for (int ll = 0; ll < NV; ll++) {
-      double a = VEC[ll], b = VEC[ll];
-      for (int ii = 0; ii < STX_NSTAGE; ii++) {
-        a = a + dt * bsv[ii] * Ks[ii * NV + ll];
-        b = b + dt * btv[ii] * Ks[ii * NV + ll];
-      }
-      ys[ll] = a;
-      errv[ll] = (b - a) / ((1.0e-4) * a + 1.0e-8);
-    }
-    double errmax = norm2v<NV>(errv);
-    double fac = 0.625 * pow(errn, 0.1) / pow(errmax, 0.175);
-    double dtnext = dt * dmin_(5.0, dmax_(0.2, fac));
-    if (errmax < 1.0) {
-      time = time + dt;
-      for (int m = 0; m < NV; m++) VEC[m] = ys[m];
-      double rho = VEC[0];
-      for (int n = 1; n < NS; n++) rho = rho + VEC[n];
-      double ri = 1.0 / rho, Y[NS];
-#pragma unroll
-      for (int n = 0; n < NS; n++) Y[n] = VEC[n] * ri;
-      double uu = VEC[NS] * ri, vv = VEC[NS + 1] * ri, ww = VEC[NS + 2] * ri;
-      double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-      double ee = VEC[NS + 3] * ri - qq;
-      T_iter = temp_from_e<NS>(c.t, c.p, ee, T_iter, Y);
-    }
-    dt = dtnext;
-    errn = errmax;
-    if (it > c.p.ros_maxsteps) { set_status(c.p, STX_ST_ROS_STEPS_CAP); break; }
-  }
-}
-
-// claim the next cell: warp-aggregated atomicAdd over the currently active lanes
-__device__ __forceinline__ long long claim(unsigned int *counter) {
-  unsigned mask = __activemask();
-  int lane = threadIdx.x & 31;
-  int leader = __ffs(mask) - 1;
-  int rank = __popc(mask & ((1u << lane) - 1u));
-  unsigned base = 0;
-  if (lane == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
-  base = __shfl_sync(mask, base, leader);
-  return (long long)base + rank;
-}
+#include "stx_chem.cuh"
 
 template <int NS>
 __global__ void __launch_bounds__(128) k_rok4(DevCtx c, double *__restrict__ w, const double *__restrict__ wa,
