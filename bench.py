@@ -195,13 +195,12 @@ def run_stx(args):
     del W, WA
     lib = sol.lib
 
+    from stx import dist as D
+
     def compute_dt_global():
         out = (C.c_double * 9)()
         check(lib.stx_compute_dt(sol.ctx, sol.stream, C.c_void_p(sol.w_aux.data_ptr()), None, out), "compute_dt")
-        m = torch.tensor(list(out), dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        sol.dt = case.cfl / float(m.max())
+        sol.dt = D.global_dt(list(out), case.cfl, device=dev)
         return sol.dt
 
     def step():
