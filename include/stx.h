@@ -42,6 +42,7 @@ extern "C" {
 #define STX_E_CUDA       -2   /* a CUDA runtime call failed */
 #define STX_E_NOMEM      -3   /* device allocation failed (stx_ctx_create only) */
 #define STX_E_UNSUPPORTED -4  /* option outside the supported hot path (e.g. IBM, LES, NR BCs) */
+#define STX_E_TOO_LARGE  -5   /* problem larger than the fixed scratch of stx_rosenbrock_krylov_noalloc */
 
 /* status bits accumulated on the device (stx_status) */
 #define STX_ST_NEWTON_CAP     0x1u  /* a Newton T(e) inversion hit its 10-iteration cap */
@@ -179,6 +180,23 @@ int stx_compute_chemistry(stx_ctx *ctx, void *stream, double *w, double *w_aux, 
  * as the reference does).  No host synchronisation inside: capture-safe. */
 int stx_rk_sync(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, int simpler);
 int stx_advance_solution(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, double time);
+
+/* Allocation-free ROK4 update, for callers that cannot call cudaMalloc (device
+ * memory owned by another runtime or a fixed pool, or a path that must not
+ * allocate while work is in flight).  No counterpart in the reference: it is
+ * stx_rosenbrock_krylov without a context.  par supplies tol_iter_nr,
+ * ros_maxsteps; tab holds DEVICE pointers to the caller's tables in the
+ * reference's layouts (kc_tab included); grid supplies nx, ny, nz, ng only.
+ * status is a device word that receives STX_ST_* bits, or NULL.
+ * Its scratch is a 4-byte file-scope device array (the work-stealing cell
+ * counter) loaded with the library on each device and kept until the process
+ * exits; it allocates nothing.  At most 2^31 cells per call (STX_E_TOO_LARGE
+ * beyond).  The first call on a device looks up the scratch's device address,
+ * so make it before any stream capture.  Calls share the scratch: each call
+ * clears it first, and calls that overlap on the GPU race on it. */
+int stx_rosenbrock_krylov_noalloc(const stx_params *par, const stx_tables *tab_dev, const stx_grid *grid,
+                                  void *stream, double *w, const double *w_aux, const double *fl_sav,
+                                  double dttry, double time_start, double time_end, int simpler, uint32_t *status);
 
 /* Device status word (OR of STX_ST_* bits since the last reset); synchronises the stream. */
 int stx_status(stx_ctx *ctx, void *stream, uint32_t *bits, int reset);

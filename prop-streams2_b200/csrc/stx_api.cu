@@ -102,6 +102,7 @@ const char *stx_strerror(int code) {
     case STX_E_CUDA: return "CUDA runtime error";
     case STX_E_NOMEM: return "device allocation failed";
     case STX_E_UNSUPPORTED: return "option outside the supported hot path";
+    case STX_E_TOO_LARGE: return "more cells than the allocation-free entry point's fixed scratch allows (2^31)";
     default: return "unknown error";
   }
 }

@@ -8,7 +8,9 @@
 // (kernels_gpu.F90:9251-9357): rhs_k += W_k sum_r (nu''_kr - nu'_kr) q_r, summed
 // over reactions in order for every species.  explicit_form selects the explicit
 // kernel's form (every species term, :9654-9661) instead of the Rosenbrock one.
-template <int NS>
+// KCF selects where K_c is read: false -> t.kc_r, the context's temperature-major
+// repacking; true -> t.kc_r in the reference's own layout kc_tab(num_t_tab+1, nr).
+template <int NS, bool KCF = false>
 __device__ void chem_source(const DevTab &t, double tt, const double *conc, double *rhs, bool explicit_form) {
   const int nr = t.nr;
   double Rtti = 1.0 / (t.Ru * tt);
@@ -69,8 +71,15 @@ __device__ void chem_source(const DevTab &t, double tt, const double *conc, doub
     }
     double kb;
     if (__ldg(t.is_rev + lr) == 1) {
-      double a = ldg(kcrow + lr);
-      double dkc = ldg(kcrow + nr + lr) - a;
+      double a, dkc;
+      if (KCF) {
+        const double *kcol = t.kc_r + (long long)lr * (t.ntab + 1) + (itt - 1);
+        a = ldg(kcol);
+        dkc = ldg(kcol + 1) - a;
+      } else {
+        a = ldg(kcrow + lr);
+        dkc = ldg(kcrow + nr + lr) - a;
+      }
       double kc = a + dkc * dtt;
       kb = kf / kc;
     } else {
@@ -106,7 +115,7 @@ __device__ void chem_source(const DevTab &t, double tt, const double *conc, doub
 }
 
 // rosenbrock_krylov_rhs (kernels_gpu.F90:10794-10976), PaSR off
-template <int NS>
+template <int NS, bool KCF = false>
 __device__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, double *rhs) {
   const DevTab &t = c.t;
   double Y[NS], conc[NS], wl[NS];
@@ -127,7 +136,7 @@ __device__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, 
   double tt = temp_from_e<NS>(t, c.p, ee, T_iter, Y);
 #pragma unroll
   for (int m = 0; m < NS + 4; m++) rhs[m] = 0.0;
-  chem_source<NS>(t, tt, conc, rhs, false);
+  chem_source<NS, KCF>(t, tt, conc, rhs, false);
 }
 
 template <int NV>
@@ -140,7 +149,7 @@ __device__ __forceinline__ double norm2v(const double *v) {
 
 // inv_matrix_krylov with ludcmp_krylov / lubksb_krylov (kernels_gpu.F90:11061-11205)
 // on the leading d x d block of a column-major 4x4 matrix.
-__device__ void inv_matrix_k(double *a, int d) {
+static __device__ void inv_matrix_k(double *a, int d) {
 #define AK(r, s) a[((s) - 1) * STX_MMAX + (r) - 1]
   if (d == 1) { AK(1, 1) = 1.0 / AK(1, 1); return; }
   int indx[STX_MMAX] = {1, 2, 3, 4};
@@ -206,7 +215,7 @@ __device__ void inv_matrix_k(double *a, int d) {
 
 // One ROK4 cell (rosenbrock_krylov_kernel body, :10463-10610).  V holds the
 // Krylov basis; the basis handed back (Vb) is its first mA columns.
-template <int NS>
+template <int NS, bool KCF = false>
 __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const double *fls, double dttry, double time_start,
                           double time_end, int simpler) {
   const int NV = NS + 4;
@@ -244,7 +253,7 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
 #pragma unroll
       for (int q = 0; q < NV * (STX_MMAX + 1); q++) V[q] = 0.0;
       mA = 0;
-      krylov_rhs<NS>(c, VEC, T_iter, rhs_sav);
+      krylov_rhs<NS, KCF>(c, VEC, T_iter, rhs_sav);
       if (simpler == 1)
         for (int m = 0; m < NV; m++) rhs_sav[m] = rhs_sav[m] - fls[m];
       double nrm = norm2v<NV>(rhs_sav);
@@ -252,7 +261,7 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
       for (int kk = 1; kk <= STX_MMAX; kk++) {
         double jac[NV], wl[NV];
         for (int m = 0; m < NV; m++) wl[m] = VEC[m] + (eps * V[(kk - 1) * NV + m]);
-        krylov_rhs<NS>(c, wl, T_iter, jac);
+        krylov_rhs<NS, KCF>(c, wl, T_iter, jac);
         if (simpler == 1)
           for (int m = 0; m < NV; m++) jac[m] = jac[m] - fls[m];
         for (int m = 0; m < NV; m++) jac[m] = (jac[m] - rhs_sav[m]) / eps;
@@ -311,7 +320,7 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
       for (int m = 0; m < NV; m++) ys[m] = VEC[m];
       for (int jj = 1; jj <= ii - 1; jj++)
         for (int m = 0; m < NV; m++) ys[m] = ys[m] + dt * alpha[ii - 1][jj - 1] * Ks[(jj - 1) * NV + m];
-      krylov_rhs<NS>(c, ys, T_iter, F);
+      krylov_rhs<NS, KCF>(c, ys, T_iter, F);
       for (int m = 0; m < NV; m++) GK[m] = 0.0;
       for (int jj = 1; jj <= ii - 1; jj++)
         for (int m = 0; m < NV; m++) GK[m] = GK[m] + gmc[ii - 1][jj - 1] / gam * Ks[(jj - 1) * NV + m];
