@@ -181,6 +181,21 @@ int stx_compute_chemistry(stx_ctx *ctx, void *stream, double *w, double *w_aux, 
 int stx_rk_sync(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, int simpler);
 int stx_advance_solution(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, double time);
 
+/* n independent adiabatic constant-pressure 0-D reactors integrated by ROK4 in
+ * one persistent launch (work stealing over reactors).  The reference's batch
+ * reactor (examples/batch_reactor, flow_init 8) is one constant-volume cell run
+ * through the whole solver; this is its batched, constant-pressure counterpart:
+ * state Y_k, h = sum Y_k h_k(T0) and p fixed, T from h by the Newton iteration of
+ * get_mixture_temperature_from_h_roe_dev (kernels_gpu.F90:6810-6900).  Device
+ * arrays: T0, p0 (n); Y0, Y (n, ns) with the reactor index fastest; outputs T,
+ * t_ign (first accepted time with T > ign_factor T0, or -1), t_end (time
+ * reached), nsteps (ROK4 steps).  Integration ends at min(t_max,
+ * end_factor t_ign); max_steps caps the steps of each reactor
+ * (STX_ST_ROS_STEPS_CAP).  Uses the context's tables and work counter. */
+int stx_batch0d_integrate(stx_ctx *ctx, void *stream, int n, const double *T0, const double *p0, const double *Y0,
+                          double t_max, double dttry, double ign_factor, double end_factor, int max_steps, double *Y,
+                          double *T, double *t_ign, double *t_end, int32_t *nsteps);
+
 /* Allocation-free ROK4 update, for callers that cannot call cudaMalloc (device
  * memory owned by another runtime or a fixed pool, or a path that must not
  * allocate while work is in flight).  No counterpart in the reference: it is

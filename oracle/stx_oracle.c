@@ -172,8 +172,14 @@ static double mix_cp(const ox_ctx *c, double tt, const double *Y) {
 }
 
 /* get_mixture_temperature_from_e_dev (kernels_gpu.F90:6532-6622); the _krylov and
- * Roe-inlined copies (:10977-11059, :3082-3157) are the same iteration. */
+ * Roe-inlined copies (:10977-11059, :3082-3157) are the same iteration.  With the
+ * cp table in place of cv it is get_mixture_temperature_from_h_roe_dev
+ * (:6810-6900), T from the mixture enthalpy. */
+static double temperature_from_poly(ox_ctx *c, const double *coef, double ee, double T_start, const double *Y);
 double ox_temperature_from_e(ox_ctx *c, double ee, double T_start, const double *Y) {
+  return temperature_from_poly(c, c->cv, ee, T_start, Y);
+}
+static double temperature_from_poly(ox_ctx *c, const double *coef, double ee, double T_start, const double *Y) {
   int nrange[MAXNS];
   int nset = c->t.nsetcv;
   const int max_iter = 10;
@@ -193,7 +199,7 @@ double ox_temperature_from_e(ox_ctx *c, double ee, double T_start, const double 
       }
     }
     double sumb = 0.0;
-    for (int lsp = 1; lsp <= NS; lsp++) sumb = sumb + CPC(c->cv, c->t.indx_cp_r + 1, lsp, nrange[lsp - 1]) * Y[lsp - 1];
+    for (int lsp = 1; lsp <= NS; lsp++) sumb = sumb + CPC(coef, c->t.indx_cp_r + 1, lsp, nrange[lsp - 1]) * Y[lsp - 1];
     double ebar = ee - sumb;
     double den = 0.0, num = 0.0;
     for (int l = c->t.indx_cp_l; l <= c->t.indx_cp_r; l++) {
@@ -206,7 +212,7 @@ double ox_temperature_from_e(ox_ctx *c, double ee, double T_start, const double 
         tnum = T_powp / (l + 1.0);
       }
       double cv_l = 0.0;
-      for (int lsp = 1; lsp <= NS; lsp++) cv_l = cv_l + CPC(c->cv, l, lsp, nrange[lsp - 1]) * Y[lsp - 1];
+      for (int lsp = 1; lsp <= NS; lsp++) cv_l = cv_l + CPC(coef, l, lsp, nrange[lsp - 1]) * Y[lsp - 1];
       num = num + cv_l * tnum;
       den = den + cv_l * tden;
     }
@@ -1389,11 +1395,26 @@ static void inv_matrix_k(double *a, int d) {
 }
 #undef AK
 
+/* The system a ROK4 integration advances: nv components, the right-hand side,
+ * and what happens after an accepted step (the temperature guess is updated;
+ * the 0-D reactor may also move the end time at ignition). */
+typedef struct ox_sys ox_sys;
+struct ox_sys {
+  ox_ctx *c;
+  int nv;
+  void (*rhs)(ox_sys *s, const double *y, double T_iter, double *out);
+  void (*accept)(ox_sys *s, const double *y, double time, double *T_iter, double *time_end);
+  /* constant-pressure reactor */
+  double p, h, T0, t_max, ign_factor, end_factor, t_ign;
+  int max_steps, nsteps;
+  double time_reached, T_final;
+};
+
 /* arnoldi (kernels_gpu.F90:10664-10792) */
-static void arnoldi(ox_ctx *c, const double *w_sav, double dt, double *Vb, double *inv, double T_iter,
+static void arnoldi(ox_sys *S, const double *w_sav, double dt, double *Vb, double *inv, double T_iter,
                     double *rhs_sav, const double *fl_sav_cell, int simpler) {
   const double gam = 0.572816062482135, TOL = 1e-6;
-  int nv = c->nv;
+  int nv = S->nv;
   double HH[(MMAX + 1) * MMAX], V[MAXNV * (MMAX + 1)], Vt[MMAX * MAXNV], HH_inv[MMAX * MMAX];
   double rhs_sav_pr[MMAX], lambda[MMAX], jac[MAXNV], wl[MAXNV], rhsp[MAXNV];
   memset(HH, 0, sizeof(HH)); memset(V, 0, sizeof(V)); memset(Vt, 0, sizeof(Vt));
@@ -1403,7 +1424,7 @@ static void arnoldi(ox_ctx *c, const double *w_sav, double dt, double *Vb, doubl
 #define Vm(r, s) V[((s) - 1) * nv + (r) - 1]
 #define VTm(r, s) Vt[((s) - 1) * MMAX + (r) - 1]
 #define HI(r, s) HH_inv[((s) - 1) * MMAX + (r) - 1]
-  krylov_rhs(c, w_sav, T_iter, rhs_sav);
+  S->rhs(S, w_sav, T_iter, rhs_sav);
   if (simpler == 1) for (int m = 0; m < nv; m++) rhs_sav[m] = rhs_sav[m] - fl_sav_cell[m];
   double nrm = norm2(rhs_sav, nv);
   for (int m = 1; m <= nv; m++) Vm(m, 1) = rhs_sav[m - 1] / nrm;
@@ -1411,7 +1432,7 @@ static void arnoldi(ox_ctx *c, const double *w_sav, double dt, double *Vb, doubl
   for (int kk = 1; kk <= MMAX; kk++) {
     /* rosenbrock_krylov_jacobian (:10613-10662) */
     for (int m = 1; m <= nv; m++) wl[m - 1] = w_sav[m - 1] + (eps * Vm(m, kk));
-    krylov_rhs(c, wl, T_iter, rhsp);
+    S->rhs(S, wl, T_iter, rhsp);
     if (simpler == 1) for (int m = 0; m < nv; m++) rhsp[m] = rhsp[m] - fl_sav_cell[m];
     for (int m = 0; m < nv; m++) jac[m] = (rhsp[m] - rhs_sav[m]) / eps;
     for (int jj = 1; jj <= kk; jj++) {
@@ -1451,13 +1472,43 @@ static void arnoldi(ox_ctx *c, const double *w_sav, double dt, double *Vb, doubl
 #undef HI
 }
 
+/* The flow cell of the reacting step: state (rho Y_k, rho u, rho v, rho w, rho E) at
+ * constant volume; after an accepted step T follows from e (:10597-10606). */
+static void flow_rhs(ox_sys *S, const double *y, double T_iter, double *out) { krylov_rhs(S->c, y, T_iter, out); }
+static void flow_accept(ox_sys *S, const double *VEC, double time, double *T_iter, double *time_end) {
+  (void)time; (void)time_end;
+  ox_ctx *c = S->c;
+  double rho = VEC[0];
+  for (int n = 2; n <= NS; n++) rho = rho + VEC[n - 1];
+  double ri = 1.0 / rho, Y[MAXNS];
+  for (int n = 1; n <= NS; n++) Y[n - 1] = VEC[n - 1] * ri;
+  double uu = VEC[NS] * ri, vv = VEC[NS + 1] * ri, ww = VEC[NS + 2] * ri;
+  double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+  double ee = VEC[NS + 3] * ri - qq;
+  *T_iter = ox_temperature_from_e(c, ee, *T_iter, Y);
+}
+
+static void rok4_core(ox_sys *S, double *VEC, double T_iter, const double *fl_sav_cell, double dttry,
+                      double time_start, double time_end, int simpler);
+
 /* rosenbrock_krylov_kernel per cell (kernels_gpu.F90:10360-10611), PaSR off.
  * The Z gate (:10464-10465) is applied by the caller. */
 void ox_krylov_cell(ox_ctx *c, double *VEC, double T_iter, double Z, const double *fl_sav_cell,
                     double dttry, double time_start, double time_end, int simpler) {
   const double eps_Z = 5e-4;
   if (!(Z > eps_Z && Z < 1.0 - eps_Z)) return;
-  int nv = c->nv;
+  ox_sys S;
+  memset(&S, 0, sizeof(S));
+  S.c = c; S.nv = c->nv; S.rhs = flow_rhs; S.accept = flow_accept; S.max_steps = c->p.ros_maxsteps;
+  rok4_core(&S, VEC, T_iter, fl_sav_cell, dttry, time_start, time_end, simpler);
+}
+
+/* The ROK4 integration of one state (the body of rosenbrock_krylov_kernel,
+ * kernels_gpu.F90:10463-10610) for the system S. */
+static void rok4_core(ox_sys *S, double *VEC, double T_iter, const double *fl_sav_cell, double dttry,
+                      double time_start, double time_end, int simpler) {
+  ox_ctx *c = S->c;
+  int nv = S->nv;
   const double gam = 0.572816062482135;
   double alpha[5][4] = {{0}}, gamma_c[5][4] = {{0}}, bs[5], bt[5];
   alpha[2][1] = 0.432364435748567;
@@ -1476,7 +1527,7 @@ void ox_krylov_cell(ox_ctx *c, double *VEC, double T_iter, double Z, const doubl
   while (time < (time_end - 1.0e-12)) {
     dt = dmin(dt, time_end - time);
     it = it + 1;
-    arnoldi(c, VEC, dt, Vb, inv, T_iter, rhs_sav, fl_sav_cell, simpler);
+    arnoldi(S, VEC, dt, Vb, inv, T_iter, rhs_sav, fl_sav_cell, simpler);
     for (int r = 1; r <= MMAX; r++)
       for (int s = 1; s <= MMAX; s++)
         IDIFF[(s - 1) * MMAX + r - 1] = (r == s ? 1.0 : 0.0) - inv[(s - 1) * MMAX + r - 1];
@@ -1496,7 +1547,7 @@ void ox_krylov_cell(ox_ctx *c, double *VEC, double T_iter, double Z, const doubl
       for (int m = 0; m < nv; m++) ys[m] = VEC[m];
       for (int jj = 1; jj <= ii - 1; jj++)
         for (int m = 0; m < nv; m++) ys[m] = ys[m] + dt * alpha[ii][jj] * Ks[(jj - 1) * nv + m];
-      krylov_rhs(c, ys, T_iter, F);
+      S->rhs(S, ys, T_iter, F);
       for (int m = 0; m < nv; m++) GK[m] = 0.0;
       for (int jj = 1; jj <= ii - 1; jj++)
         for (int m = 0; m < nv; m++) GK[m] = GK[m] + gamma_c[ii][jj] / gam * Ks[(jj - 1) * nv + m];
@@ -1524,22 +1575,18 @@ void ox_krylov_cell(ox_ctx *c, double *VEC, double T_iter, double Z, const doubl
     if (errmax < 1.0) {
       time = time + dt;
       for (int m = 0; m < nv; m++) VEC[m] = ys[m];
-      double rho = VEC[0];
-      for (int n = 2; n <= NS; n++) rho = rho + VEC[n - 1];
-      double ri = 1.0 / rho, Y[MAXNS];
-      for (int n = 1; n <= NS; n++) Y[n - 1] = VEC[n - 1] * ri;
-      double uu = VEC[NS] * ri, vv = VEC[NS + 1] * ri, ww = VEC[NS + 2] * ri;
-      double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-      double ee = VEC[NS + 3] * ri - qq;
-      T_iter = ox_temperature_from_e(c, ee, T_iter, Y);
+      S->accept(S, VEC, time, &T_iter, &time_end);
       dt = dtnext;
       errn = errmax;
     } else {
       dt = dtnext;
       errn = errmax;
     }
-    if (it > c->p.ros_maxsteps) { c->status |= STX_ST_ROS_STEPS_CAP; break; }
+    if (it > S->max_steps) { c->status |= STX_ST_ROS_STEPS_CAP; break; }
   }
+  S->nsteps = it;
+  S->time_reached = time;
+  S->T_final = T_iter;
 }
 
 void ox_rosenbrock_krylov(ox_ctx *c, double *w, const double *wa, const double *fl_sav, double dttry,
@@ -1561,6 +1608,65 @@ void ox_rosenbrock_krylov(ox_ctx *c, double *w, const double *wa, const double *
           for (int m = 1; m <= nv; m++) WG(w, p, m) = VEC[m - 1];
         }
       }
+}
+
+/* ---- 0-D adiabatic constant-pressure reactors.  The reference's batch reactor
+ * (examples/batch_reactor) is constant-volume; the constant-pressure form has no
+ * counterpart there.  State Y_k (clipped at 0 where evaluated); h = sum Y_k h_k(T0)
+ * and p stay fixed; T follows from h by the Newton iteration of
+ * get_mixture_temperature_from_h_roe_dev (kernels_gpu.F90:6810-6900); rho = p/(R T);
+ * dY_k/dt = W_k omega_k / rho with the production rates of rosenbrock_krylov_rhs
+ * (:10794-10976), integrated by the same ROK4 scheme.  After the first accepted
+ * step with T > ign_factor T0 (the ignition time t_ign, as mech_comp.py's
+ * T > 1.05 T0 test) the end time becomes min(t_max, end_factor t_ign). */
+static void cp_rhs(ox_sys *S, const double *y, double T_iter, double *out) {
+  ox_ctx *c = S->c;
+  double Yc[MAXNS], conc[MAXNS], qlr[512];
+  for (int k = 0; k < NS; k++) Yc[k] = dmax(y[k], 0.0);
+  double tt = temperature_from_poly(c, c->cp, S->h, T_iter, Yc);
+  double rm = 0.0;
+  for (int k = 0; k < NS; k++) rm = rm + c->rgas[k] * Yc[k];
+  double rho = S->p / (rm * tt);
+  for (int k = 0; k < NS; k++) conc[k] = rho * Yc[k] / c->mw[k];
+  for (int k = 0; k < NS; k++) out[k] = 0.0;
+  reaction_rates(c, tt, conc, qlr);
+  species_rhs(c, qlr, out);
+  for (int k = 0; k < NS; k++) out[k] = out[k] / rho;
+}
+
+static void cp_accept(ox_sys *S, const double *y, double time, double *T_iter, double *time_end) {
+  ox_ctx *c = S->c;
+  double Yc[MAXNS];
+  for (int k = 0; k < NS; k++) Yc[k] = dmax(y[k], 0.0);
+  *T_iter = temperature_from_poly(c, c->cp, S->h, *T_iter, Yc);
+  if (S->t_ign < 0.0 && *T_iter > S->ign_factor * S->T0) {
+    S->t_ign = time;
+    double te = S->end_factor * time;
+    if (te < *time_end) *time_end = te;
+  }
+}
+
+void ox_batch0d_cp(ox_ctx *c, int n, const double *T0, const double *p0, const double *Y0, double t_max,
+                   double dttry, double ign_factor, double end_factor, int max_steps, double *Y, double *T,
+                   double *t_ign, double *t_end, int32_t *nsteps) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int r = 0; r < n; r++) {
+    ox_sys S;
+    memset(&S, 0, sizeof(S));
+    S.c = c; S.nv = NS; S.rhs = cp_rhs; S.accept = cp_accept; S.max_steps = max_steps;
+    double VEC[MAXNS];
+    for (int k = 0; k < NS; k++) VEC[k] = Y0[(size_t)k * n + r];
+    double h = 0.0;
+    for (int k = 0; k < NS; k++) h = h + VEC[k] * species_poly_int(c, c->cp, T0[r], k + 1);
+    S.h = h; S.p = p0[r]; S.T0 = T0[r]; S.t_max = t_max;
+    S.ign_factor = ign_factor; S.end_factor = end_factor; S.t_ign = -1.0;
+    rok4_core(&S, VEC, T0[r], NULL, dttry, 0.0, t_max, 0);
+    for (int k = 0; k < NS; k++) Y[(size_t)k * n + r] = VEC[k];
+    T[r] = S.T_final;
+    t_ign[r] = S.t_ign;
+    t_end[r] = S.time_reached;
+    nsteps[r] = S.nsteps;
+  }
 }
 
 /* ---- full-Jacobian Rosenbrock (kernels_gpu.F90:8928-9501), one cell.  The cell

@@ -60,6 +60,12 @@ void ox_rosenbrock_cell(ox_ctx *c, double *wcell, double *Y, double *T, double d
                         double time_start, double time_end);
 double ox_temperature_from_e(ox_ctx *c, double ee, double T_start, const double *Y);
 
+/* n adiabatic constant-pressure 0-D reactors (the batched-reactor workload);
+ * Y0 / Y are (n, ns) with the reactor index fastest */
+void ox_batch0d_cp(ox_ctx *c, int n, const double *T0, const double *p0, const double *Y0, double t_max,
+                   double dttry, double ign_factor, double end_factor, int max_steps, double *Y, double *T,
+                   double *t_ign, double *t_end, int32_t *nsteps);
+
 #ifdef __cplusplus
 }
 #endif

@@ -194,6 +194,38 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
     if ((rc = upload(c, tab->tb_eff, (size_t)nr * ns, &t.tb_eff))) return fail(rc);
     if ((rc = upload(c, tab->r_coeffs, (size_t)nr * ns, &t.r_coeffs))) return fail(rc);
     if ((rc = upload(c, tab->p_coeffs, (size_t)nr * ns, &t.p_coeffs))) return fail(rc);
+    {
+      // sparse stoichiometry: the species with nonzero nu' / nu'' of each
+      // reaction, ascending, so the rate kernels visit exactly the terms the
+      // dense species loops would, in the same order
+      std::vector<int> cnt(nr);
+      std::vector<unsigned char> idx((size_t)nr * STX_SPW, 0);
+      std::vector<double> coef((size_t)nr * STX_SPW, 0.0);
+      for (int r = 0; r < nr; r++) {
+        int nR = 0, nP = 0, nU = 0;
+        for (int k = 0; k < ns; k++) {
+          double rr = tab->r_coeffs[(size_t)k * nr + r], pp = tab->p_coeffs[(size_t)k * nr + r];
+          if (rr != 0.0) {
+            if (nR == STX_SPR) return fail(STX_E_UNSUPPORTED);
+            idx[(size_t)r * STX_SPW + nR] = (unsigned char)k;
+            coef[(size_t)r * STX_SPW + nR++] = rr;
+          }
+          if (pp != 0.0) {
+            if (nP == STX_SPR) return fail(STX_E_UNSUPPORTED);
+            idx[(size_t)r * STX_SPW + STX_SPR + nP] = (unsigned char)k;
+            coef[(size_t)r * STX_SPW + STX_SPR + nP++] = pp;
+          }
+          if (rr != 0.0 || pp != 0.0) {
+            idx[(size_t)r * STX_SPW + 2 * STX_SPR + nU] = (unsigned char)k;
+            coef[(size_t)r * STX_SPW + 2 * STX_SPR + nU++] = pp - rr;
+          }
+        }
+        cnt[r] = nR | (nP << 8) | (nU << 16);
+      }
+      if ((rc = upload(c, cnt.data(), cnt.size(), &t.sp_cnt))) return fail(rc);
+      if ((rc = upload(c, idx.data(), idx.size(), &t.sp_idx))) return fail(rc);
+      if ((rc = upload(c, coef.data(), coef.size(), &t.sp_coef))) return fail(rc);
+    }
     std::vector<double> kr(ntab1 * nr);
     for (size_t it = 0; it < ntab1; it++)
       for (int r = 0; r < nr; r++) kr[it * nr + r] = tab->kc_tab[(size_t)r * ntab1 + it];
@@ -423,6 +455,18 @@ int stx_rosenbrock_krylov(stx_ctx *c, void *s, double *w, const double *wa, cons
   if (c->d.t.nr < 1) return STX_E_INVALID;
   Prof pf(c, S(s), STX_K_CHEM, 1, (double)c->d.g.npi * B8(2 * c->nv + 2));
   return launch_rok4(c->d, S(s), w, wa, fl_sav, dttry, t0, t1, simpler, c->counter_d);
+}
+int stx_batch0d_integrate(stx_ctx *c, void *s, int n, const double *T0, const double *p0, const double *Y0,
+                          double t_max, double dttry, double ign_factor, double end_factor, int max_steps, double *Y,
+                          double *T, double *t_ign, double *t_end, int32_t *nsteps) {
+  if (!c || n < 0 || (n > 0 && (!T0 || !p0 || !Y0 || !Y || !T || !t_ign || !t_end || !nsteps))) return STX_E_INVALID;
+  if (c->d.t.nr < 1 || !(t_max > 0.0) || !(dttry > 0.0) || max_steps < 1) return STX_E_INVALID;
+  if (n == 0) return STX_OK;
+  DevCtx d = c->d;
+  d.p.ros_maxsteps = max_steps;
+  Prof pf(c, S(s), STX_K_CHEM, 1, (double)n * 8.0 * (2 * c->d.t.ns + 6));
+  return launch_batch0d(d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end, nsteps,
+                        c->counter_d);
 }
 int stx_compute_chemistry(stx_ctx *c, void *s, double *w, double *wa, double *fl) {
   if (!c || !w || !wa || !fl) return STX_E_INVALID;

@@ -13,8 +13,14 @@
 // the FP64 oracle operation by operation (libm vs CUDA exp/pow/log10 aside).
 #include "stx_chem.cuh"
 
+// CTAs per SM the ROK4 kernel's register budget is sized for
+#ifndef STX_ROK4_MINB
+#define STX_ROK4_MINB 4
+#endif
+
 template <int NS>
-__global__ void __launch_bounds__(128) k_rok4(DevCtx c, double *__restrict__ w, const double *__restrict__ wa,
+__global__ void __launch_bounds__(STX_CHEM_BLOCK, STX_ROK4_MINB)
+    k_rok4(DevCtx c, double *__restrict__ w, const double *__restrict__ wa,
                                               const double *__restrict__ fl_sav, double dttry, double t0, double t1,
                                               int simpler, unsigned int *counter) {
   const DevGrid &g = c.g;
@@ -39,6 +45,37 @@ __global__ void __launch_bounds__(128) k_rok4(DevCtx c, double *__restrict__ w, 
     rok4_cell<NS>(c, VEC, FG(wa, p, NS + 5), fls, dttry, t0, t1, simpler);
 #pragma unroll
     for (int m = 0; m < NV; m++) FG(w, p, m + 1) = VEC[m];
+  }
+}
+
+// n independent adiabatic constant-pressure 0-D reactors, one thread each,
+// claimed from the work-stealing counter (reactors ignite at very different
+// times, so their step counts differ by orders of magnitude).  Y0 / Y are
+// (n, ns) with the reactor index fastest.
+template <int NS>
+__global__ void __launch_bounds__(STX_CHEM_BLOCK, STX_ROK4_MINB)
+    k_batch0d(DevCtx c, int n, const double *__restrict__ T0, const double *__restrict__ p0,
+              const double *__restrict__ Y0, double t_max, double dttry, double ign_factor, double end_factor,
+              double *__restrict__ Y, double *__restrict__ T, double *__restrict__ t_ign, double *__restrict__ t_end,
+              int *__restrict__ nsteps, unsigned int *counter) {
+  for (;;) {
+    long long r = claim(counter);
+    if (r >= n) break;
+    double VEC[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) VEC[k] = Y0[(long long)k * n + r];
+    const double T0r = T0[r];
+    double h = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < NS; k++) h = h + VEC[k] * species_poly_int(c.t, c.t.cp, T0r, k + 1);
+    Rok4ConstP<NS> f{c, h, p0[r], T0r, ign_factor, end_factor, -1.0, 0.0, T0r, 0};
+    rok4_core<NS>(c, f, VEC, T0r, nullptr, dttry, 0.0, t_max, 0);
+#pragma unroll
+    for (int k = 0; k < NS; k++) Y[(long long)k * n + r] = VEC[k];
+    T[r] = f.T_final;
+    t_ign[r] = f.t_ign;
+    t_end[r] = f.time_reached;
+    nsteps[r] = f.steps;
   }
 }
 
@@ -285,10 +322,10 @@ template <int NS>
 static int rok4_t(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
                   double t0, double t1, int simpler, unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
-  int nb = persistent_blocks((const void *)k_rok4<NS>, 128);
-  long long need = (c.g.npi + 127) / 128;
+  int nb = persistent_blocks((const void *)k_rok4<NS>, STX_CHEM_BLOCK);
+  long long need = (c.g.npi + STX_CHEM_BLOCK - 1) / STX_CHEM_BLOCK;
   if (nb > need) nb = (int)need;
-  k_rok4<NS><<<nb, 128, 0, s>>>(c, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
+  k_rok4<NS><<<nb, STX_CHEM_BLOCK, 0, s>>>(c, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
@@ -309,6 +346,31 @@ int launch_rok4(const DevCtx &c, cudaStream_t s, double *w, const double *wa, co
                 double t0, double t1, int simpler, unsigned int *counter) {
   switch (c.t.ns) {
 #define X(N) case N: return rok4_t<N>(c, s, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
+}
+
+template <int NS>
+static int batch0d_t(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
+                     double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
+                     double *t_end, int *nsteps, unsigned int *counter) {
+  STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
+  int nb = persistent_blocks((const void *)k_batch0d<NS>, STX_CHEM_BLOCK);
+  long long need = ((long long)n + STX_CHEM_BLOCK - 1) / STX_CHEM_BLOCK;
+  if (nb > need) nb = (int)need;
+  k_batch0d<NS><<<nb, STX_CHEM_BLOCK, 0, s>>>(c, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps,
+                                              counter);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
+                   double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
+                   double *t_end, int *nsteps, unsigned int *counter) {
+  switch (c.t.ns) {
+#define X(N) case N: return batch0d_t<N>(c, s, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps, counter);
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;

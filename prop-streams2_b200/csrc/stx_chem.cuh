@@ -4,87 +4,109 @@
 #pragma once
 #include "stx_kernels.cuh"
 
+// Threads per CTA of the chemistry kernels (per-thread shared-memory rows).
+#define STX_CHEM_BLOCK 128
+
+// Temperature-table position of T for K_c (kernels_gpu.F90:9259-9264).
+__device__ __forceinline__ void kc_pos(const DevTab &t, double tt, int &itt, double &dtt) {
+  itt = (int)((tt - t.tmin) / t.dtab) + 1;
+  if (itt < 1) itt = 1;
+  if (itt > t.ntab) itt = t.ntab;
+  double ttleft = (itt - 1) * t.dtab + t.tmin;
+  dtt = (tt - ttleft) / t.dtab;
+}
+
+// Rate constants of reaction lr at T (kernels_gpu.F90:9266-9330): kf from the
+// Arrhenius, Lindemann, Troe or SRI form (tbs is the third-body concentration
+// sum the fall-off forms use), kb = kf / K_c with K_c interpolated in the 1-K
+// table.  KCF selects where K_c is read: false -> t.kc_r, the context's
+// temperature-major repacking; true -> t.kc_r in the reference's own layout
+// kc_tab(num_t_tab+1, nr).
+template <bool KCF>
+__device__ __forceinline__ void rate_consts(const DevTab &t, int lr, int ty, double tt, double Rtti, int itt,
+                                            double dtt, double tbs, double &kf, double &kb) {
+  const int nr = t.nr;
+  double A1 = ldg(t.arr_a + lr), B1 = ldg(t.arr_b + lr), E1 = ldg(t.arr_ea + lr);
+  if (ty == 0 || ty == 1) {
+    kf = A1;
+    if (B1 != 0.0) kf = kf * pow(tt, B1);
+    if (E1 != 0.0) kf = kf * exp(-E1 * Rtti);
+  } else {
+    double A2 = ldg(t.arr_a + nr + lr), B2 = ldg(t.arr_b + nr + lr), E2 = ldg(t.arr_ea + nr + lr);
+    double k0 = A1 * pow(tt, B1) * exp(-E1 * Rtti);
+    double kinf = A2 * pow(tt, B2) * exp(-E2 * Rtti);
+    double rpres = k0 * tbs / kinf;
+    if (ty == 2) {
+      kf = kinf * (rpres / (1.0 + rpres));
+    } else if (ty == 3) {
+      if (rpres < 1e-30) {
+        kf = k0 * tbs;
+      } else {
+        double F1 = ldg(t.falloff + lr), F2 = ldg(t.falloff + nr + lr), F3 = ldg(t.falloff + 2 * nr + lr),
+               F4 = ldg(t.falloff + 3 * nr + lr);
+        double fcent = (1.0 - F1) * exp(-tt / F2) + F1 * exp(-tt / F3);
+        if (F4 != -3.14) fcent = fcent + exp(-F4 / tt);
+        fcent = log10(fcent);
+        double coff = -0.4 - 0.67 * fcent;
+        double noff = 0.75 - 1.27 * fcent;
+        double doff = 0.14;
+        double lp = log10(rpres);
+        double foff = pow(10.0, pow(1.0 + pow((lp + coff) / (noff - doff * (lp + coff)), 2.0), -1.0) * fcent);
+        kf = kinf * (rpres / (1.0 + rpres)) * foff;
+      }
+    } else if (ty == 4) {
+      double F1 = ldg(t.falloff + lr), F2 = ldg(t.falloff + nr + lr), F3 = ldg(t.falloff + 2 * nr + lr),
+             F4 = ldg(t.falloff + 3 * nr + lr), F5 = ldg(t.falloff + 4 * nr + lr);
+      double xoff = 1.0 / (1.0 + pow(log10(rpres), 2.0));
+      double foff = F4 * pow(F1 * exp(-F2 / tt) + exp(-tt / F3), xoff) * pow(tt, F5);
+      kf = kinf * (rpres / (1.0 + rpres)) * foff;
+    } else {
+      kf = 0.0;
+    }
+  }
+  if (__ldg(t.is_rev + lr) == 1) {
+    double a, dkc;
+    if (KCF) {
+      const double *kcol = t.kc_r + (long long)lr * (t.ntab + 1) + (itt - 1);
+      a = ldg(kcol);
+      dkc = ldg(kcol + 1) - a;
+    } else {
+      const double *kcrow = t.kc_r + (long long)(itt - 1) * nr;
+      a = ldg(kcrow + lr);
+      dkc = ldg(kcrow + nr + lr) - a;
+    }
+    double kc = a + dkc * dtt;
+    kb = kf / kc;
+  } else {
+    kb = 0.0;
+  }
+}
+
 // Production terms of rosenbrock_rhs / rosenbrock_krylov_rhs / compute_chemistry_cuf
 // (kernels_gpu.F90:9251-9357): rhs_k += W_k sum_r (nu''_kr - nu'_kr) q_r, summed
-// over reactions in order for every species.  explicit_form selects the explicit
-// kernel's form (every species term, :9654-9661) instead of the Rosenbrock one.
-// KCF selects where K_c is read: false -> t.kc_r, the context's temperature-major
-// repacking; true -> t.kc_r in the reference's own layout kc_tab(num_t_tab+1, nr).
+// over reactions in order for every species, with dense species loops.
+// explicit_form selects the explicit kernel's form (every species term,
+// :9654-9661) instead of the Rosenbrock one.  The third-body sum is the sum
+// the reference forms in its fall-off branch and again for three-body
+// reactions; it is formed once here (same terms, same order, same value).
 template <int NS, bool KCF = false>
 __device__ void chem_source(const DevTab &t, double tt, const double *conc, double *rhs, bool explicit_form) {
   const int nr = t.nr;
   double Rtti = 1.0 / (t.Ru * tt);
   int itt;
   double dtt;
-  {
-    itt = (int)((tt - t.tmin) / t.dtab) + 1;
-    if (itt < 1) itt = 1;
-    if (itt > t.ntab) itt = t.ntab;
-    double ttleft = (itt - 1) * t.dtab + t.tmin;
-    dtt = (tt - ttleft) / t.dtab;
-  }
-  const double *kcrow = t.kc_r + (long long)(itt - 1) * nr;
+  kc_pos(t, tt, itt, dtt);
 #pragma unroll 1
   for (int lr = 0; lr < nr; lr++) {
     int ty = __ldg(t.reac_ty + lr);
-    double kf, k0, kinf, tb, rpres;
-    double A1 = ldg(t.arr_a + lr), B1 = ldg(t.arr_b + lr), E1 = ldg(t.arr_ea + lr);
-    if (ty == 0 || ty == 1) {
-      kf = A1;
-      if (B1 != 0.0) kf = kf * pow(tt, B1);
-      if (E1 != 0.0) kf = kf * exp(-E1 * Rtti);
-    } else {
-      double A2 = ldg(t.arr_a + nr + lr), B2 = ldg(t.arr_b + nr + lr), E2 = ldg(t.arr_ea + nr + lr);
-      k0 = A1 * pow(tt, B1) * exp(-E1 * Rtti);
-      kinf = A2 * pow(tt, B2) * exp(-E2 * Rtti);
-      tb = 0.0;
+    double tbs = 1.0;
+    if (ty != 0) {
+      tbs = 0.0;
 #pragma unroll
-      for (int k = 0; k < NS; k++) tb = tb + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k];
-      rpres = k0 * tb / kinf;
-      if (ty == 2) {
-        kf = kinf * (rpres / (1.0 + rpres));
-      } else if (ty == 3) {
-        if (rpres < 1e-30) {
-          kf = k0 * tb;
-        } else {
-          double F1 = ldg(t.falloff + lr), F2 = ldg(t.falloff + nr + lr), F3 = ldg(t.falloff + 2 * nr + lr),
-                 F4 = ldg(t.falloff + 3 * nr + lr);
-          double fcent = (1.0 - F1) * exp(-tt / F2) + F1 * exp(-tt / F3);
-          if (F4 != -3.14) fcent = fcent + exp(-F4 / tt);
-          fcent = log10(fcent);
-          double coff = -0.4 - 0.67 * fcent;
-          double noff = 0.75 - 1.27 * fcent;
-          double doff = 0.14;
-          double lp = log10(rpres);
-          double foff = pow(10.0, pow(1.0 + pow((lp + coff) / (noff - doff * (lp + coff)), 2.0), -1.0) * fcent);
-          kf = kinf * (rpres / (1.0 + rpres)) * foff;
-        }
-      } else if (ty == 4) {
-        double F1 = ldg(t.falloff + lr), F2 = ldg(t.falloff + nr + lr), F3 = ldg(t.falloff + 2 * nr + lr),
-               F4 = ldg(t.falloff + 3 * nr + lr), F5 = ldg(t.falloff + 4 * nr + lr);
-        double xoff = 1.0 / (1.0 + pow(log10(rpres), 2.0));
-        double foff = F4 * pow(F1 * exp(-F2 / tt) + exp(-tt / F3), xoff) * pow(tt, F5);
-        kf = kinf * (rpres / (1.0 + rpres)) * foff;
-      } else {
-        kf = 0.0;
-      }
+      for (int k = 0; k < NS; k++) tbs = tbs + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k];
     }
-    double kb;
-    if (__ldg(t.is_rev + lr) == 1) {
-      double a, dkc;
-      if (KCF) {
-        const double *kcol = t.kc_r + (long long)lr * (t.ntab + 1) + (itt - 1);
-        a = ldg(kcol);
-        dkc = ldg(kcol + 1) - a;
-      } else {
-        a = ldg(kcrow + lr);
-        dkc = ldg(kcrow + nr + lr) - a;
-      }
-      double kc = a + dkc * dtt;
-      kb = kf / kc;
-    } else {
-      kb = 0.0;
-    }
+    double kf, kb;
+    rate_consts<KCF>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb);
     double q1 = 1.0, q2 = 1.0;
 #pragma unroll
     for (int k = 0; k < NS; k++) {
@@ -94,12 +116,7 @@ __device__ void chem_source(const DevTab &t, double tt, const double *conc, doub
       if (pp == 1.0) q2 = q2 * conc[k];
       else if (pp != 0.0) q2 = q2 * pow(conc[k], pp);
     }
-    tb = 1.0;
-    if (ty == 1) {
-      tb = 0.0;
-#pragma unroll
-      for (int k = 0; k < NS; k++) tb = tb + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k];
-    }
+    double tb = (ty == 1) ? tbs : 1.0;
     double qlr = tb * (kf * q1 - kb * q2);
 #pragma unroll
     for (int k = 0; k < NS; k++) {
@@ -114,9 +131,63 @@ __device__ void chem_source(const DevTab &t, double tt, const double *conc, doub
   }
 }
 
-// rosenbrock_krylov_rhs (kernels_gpu.F90:10794-10976), PaSR off
+// The Rosenbrock-form production terms of chem_source over the sparse
+// stoichiometry lists (t.sp_*): the same terms in the same order, with compact
+// rolled loops.  conc and rhs are per-thread rows with stride S (shared memory).
+template <int NS, int S>
+__device__ void chem_source_sp(const DevTab &t, double tt, const double *conc, double *rhs) {
+  const int nr = t.nr;
+  double Rtti = 1.0 / (t.Ru * tt);
+  int itt;
+  double dtt;
+  kc_pos(t, tt, itt, dtt);
+#pragma unroll 1
+  for (int lr = 0; lr < nr; lr++) {
+    int ty = __ldg(t.reac_ty + lr);
+    double tbs = 1.0;
+    if (ty != 0) {
+      tbs = 0.0;
+#pragma unroll 1
+      for (int k = 0; k < NS; k++) tbs = tbs + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k * S];
+    }
+    double kf, kb;
+    rate_consts<false>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb);
+    const int cnt = __ldg(t.sp_cnt + lr);
+    const unsigned char *ix = t.sp_idx + (long long)lr * STX_SPW;
+    const double *cf = t.sp_coef + (long long)lr * STX_SPW;
+    double q1 = 1.0, q2 = 1.0;
+#pragma unroll 1
+    for (int n = 0; n < (cnt & 255); n++) {
+      double x = conc[__ldg(ix + n) * S], e = ldg(cf + n);
+      if (e == 1.0) q1 = q1 * x;
+      else q1 = q1 * pow(x, e);
+    }
+#pragma unroll 1
+    for (int n = 0; n < ((cnt >> 8) & 255); n++) {
+      double x = conc[__ldg(ix + STX_SPR + n) * S], e = ldg(cf + STX_SPR + n);
+      if (e == 1.0) q2 = q2 * x;
+      else q2 = q2 * pow(x, e);
+    }
+    double tb = (ty == 1) ? tbs : 1.0;
+    double qlr = tb * (kf * q1 - kb * q2);
+#pragma unroll 1
+    for (int n = 0; n < (cnt >> 16); n++) {
+      int k = __ldg(ix + 2 * STX_SPR + n);
+      double wdtkj = ldg(cf + 2 * STX_SPR + n) * qlr;
+      rhs[k * S] = rhs[k * S] + wdtkj * ldg(t.mw + k);
+    }
+  }
+}
+
+// rosenbrock_krylov_rhs (kernels_gpu.F90:10794-10976), PaSR off.  Kept out of
+// line: one copy serves the Arnoldi, Jacobian-vector and stage evaluations, so
+// the ROK4 loop stays small enough for the instruction cache.  With the
+// context's tables (KCF false) the production terms run over the sparse
+// stoichiometry with per-thread rows in shared memory (launch with
+// STX_CHEM_BLOCK threads); with the reference's raw tables (KCF true) over the
+// dense species loops.
 template <int NS, bool KCF = false>
-__device__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, double *rhs) {
+__device__ __noinline__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, double *rhs) {
   const DevTab &t = c.t;
   double Y[NS], conc[NS], wl[NS];
 #pragma unroll
@@ -136,7 +207,20 @@ __device__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, 
   double tt = temp_from_e<NS>(t, c.p, ee, T_iter, Y);
 #pragma unroll
   for (int m = 0; m < NS + 4; m++) rhs[m] = 0.0;
-  chem_source<NS, KCF>(t, tt, conc, rhs, false);
+  if (KCF) {
+    chem_source<NS, KCF>(t, tt, conc, rhs, false);
+  } else {
+    __shared__ double s_conc[NS * STX_CHEM_BLOCK], s_rhs[NS * STX_CHEM_BLOCK];
+    double *cs = s_conc + threadIdx.x, *rs = s_rhs + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      cs[k * STX_CHEM_BLOCK] = conc[k];
+      rs[k * STX_CHEM_BLOCK] = 0.0;
+    }
+    chem_source_sp<NS, STX_CHEM_BLOCK>(t, tt, cs, rs);
+#pragma unroll
+    for (int k = 0; k < NS; k++) rhs[k] = rs[k * STX_CHEM_BLOCK];
+  }
 }
 
 template <int NV>
@@ -213,12 +297,17 @@ static __device__ void inv_matrix_k(double *a, int d) {
 #undef AK
 }
 
-// One ROK4 cell (rosenbrock_krylov_kernel body, :10463-10610).  V holds the
-// Krylov basis; the basis handed back (Vb) is its first mA columns.
-template <int NS, bool KCF = false>
-__device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const double *fls, double dttry, double time_start,
-                          double time_end, int simpler) {
-  const int NV = NS + 4;
+// The ROK4 integration of one state vector of NV components
+// (rosenbrock_krylov_kernel body, kernels_gpu.F90:10463-10610).  V holds the
+// Krylov basis; the basis handed back (Vb) is its first mA columns.  The
+// system is the functor f:
+//   f.rhs(y, T_iter, out)               the right-hand side at y;
+//   f.accept(y, time, T_iter, time_end) after an accepted step: updates the
+//                                       temperature guess, may move time_end;
+//   f.done(time, T_iter, steps)         at the end: time reached, last T, steps.
+template <int NV, class F>
+__device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, const double *fls, double dttry,
+                          double time_start, double time_end, int simpler) {
   const double gam = 0.572816062482135;
   const double a21 = 0.432364435748567, a31 = -0.514211316876170, a32 = 1.382271144617360;
   const double a41 = -0.514211316876170, a42 = 1.382271144617360, a43 = 0.0;
@@ -253,18 +342,22 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
 #pragma unroll
       for (int q = 0; q < NV * (STX_MMAX + 1); q++) V[q] = 0.0;
       mA = 0;
-      krylov_rhs<NS, KCF>(c, VEC, T_iter, rhs_sav);
+      f.rhs(VEC, T_iter, rhs_sav);
       if (simpler == 1)
         for (int m = 0; m < NV; m++) rhs_sav[m] = rhs_sav[m] - fls[m];
       double nrm = norm2v<NV>(rhs_sav);
       for (int m = 0; m < NV; m++) V[m] = rhs_sav[m] / nrm;
+      // the outer loops stay rolled (unroll 1): unrolled, the Krylov algebra
+      // is straight-line code far larger than the instruction cache
+#pragma unroll 1
       for (int kk = 1; kk <= STX_MMAX; kk++) {
         double jac[NV], wl[NV];
         for (int m = 0; m < NV; m++) wl[m] = VEC[m] + (eps * V[(kk - 1) * NV + m]);
-        krylov_rhs<NS, KCF>(c, wl, T_iter, jac);
+        f.rhs(wl, T_iter, jac);
         if (simpler == 1)
           for (int m = 0; m < NV; m++) jac[m] = jac[m] - fls[m];
         for (int m = 0; m < NV; m++) jac[m] = (jac[m] - rhs_sav[m]) / eps;
+#pragma unroll 1
         for (int jj = 1; jj <= kk; jj++) {
           double dot = 0.0;
           for (int m = 0; m < NV; m++) dot = dot + V[(jj - 1) * NV + m] * jac[m];
@@ -275,13 +368,16 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
         HH[(kk - 1) * (STX_MMAX + 1) + kk] = hn;
         for (int m = 0; m < NV; m++) V[kk * NV + m] = jac[m] / hn;
         // projections of rhs_sav on the first kk basis vectors (the rest are zero)
+#pragma unroll 1
         for (int ll = 1; ll <= STX_MMAX; ll++) {
           double s = 0.0;
           if (ll <= kk)
             for (int m = 0; m < NV; m++) s = s + V[(ll - 1) * NV + m] * rhs_sav[m];
           prj[ll - 1] = s;
         }
+#pragma unroll 1
         for (int n = 1; n <= kk; n++)
+#pragma unroll 1
           for (int nn = 1; nn <= kk; nn++) {
             double h = -(dt * gam * HH[(nn - 1) * (STX_MMAX + 1) + n - 1]);
             if (n == nn) h = h + 1.0;
@@ -303,7 +399,9 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
       }
     }
     // ---- A = Vb (I - inv)  (Vb = first mA columns of V, zero beyond)
+#pragma unroll 1
     for (int kk = 1; kk <= STX_MMAX; kk++)
+#pragma unroll 1
       for (int ll = 0; ll < NV; ll++) {
         double idf = ((1 == kk) ? 1.0 : 0.0) - inv[(kk - 1) * STX_MMAX + 0];
         double a = (mA >= 1 ? V[ll] : 0.0) * idf;
@@ -315,18 +413,22 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
         Am[(kk - 1) * NV + ll] = a;
       }
     // ---- stages; B(ll,jj) = sum_q A(ll,q) Vb(jj,q) is recomputed where used
+#pragma unroll 1
     for (int ii = 1; ii <= STX_NSTAGE; ii++) {
       double ys[NV], F[NV], GK[NV];
       for (int m = 0; m < NV; m++) ys[m] = VEC[m];
+#pragma unroll 1
       for (int jj = 1; jj <= ii - 1; jj++)
         for (int m = 0; m < NV; m++) ys[m] = ys[m] + dt * alpha[ii - 1][jj - 1] * Ks[(jj - 1) * NV + m];
-      krylov_rhs<NS, KCF>(c, ys, T_iter, F);
+      f.rhs(ys, T_iter, F);
       for (int m = 0; m < NV; m++) GK[m] = 0.0;
+#pragma unroll 1
       for (int jj = 1; jj <= ii - 1; jj++)
         for (int m = 0; m < NV; m++) GK[m] = GK[m] + gmc[ii - 1][jj - 1] / gam * Ks[(jj - 1) * NV + m];
       for (int m = 0; m < NV; m++) F[m] = F[m] + GK[m];
       if (simpler == 1)
         for (int m = 0; m < NV; m++) F[m] = F[m] - fls[m];
+#pragma unroll 1
       for (int ll = 0; ll < NV; ll++) {
         double s = 0.0;
         for (int jj = 0; jj < NV; jj++) {
@@ -353,20 +455,101 @@ __device__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const dou
     if (errmax < 1.0) {
       time = time + dt;
       for (int m = 0; m < NV; m++) VEC[m] = ys[m];
-      double rho = VEC[0];
-      for (int n = 1; n < NS; n++) rho = rho + VEC[n];
-      double ri = 1.0 / rho, Y[NS];
-#pragma unroll
-      for (int n = 0; n < NS; n++) Y[n] = VEC[n] * ri;
-      double uu = VEC[NS] * ri, vv = VEC[NS + 1] * ri, ww = VEC[NS + 2] * ri;
-      double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-      double ee = VEC[NS + 3] * ri - qq;
-      T_iter = temp_from_e<NS>(c.t, c.p, ee, T_iter, Y);
+      f.accept(VEC, time, T_iter, time_end);
     }
     dt = dtnext;
     errn = errmax;
     if (it > c.p.ros_maxsteps) { set_status(c.p, STX_ST_ROS_STEPS_CAP); break; }
   }
+  f.done(time, T_iter, it);
+}
+
+// The flow cell: state (rho Y_k, rho u, rho v, rho w, rho E), constant volume
+// (rosenbrock_krylov_rhs, :10794-10976); after an accepted step T follows from
+// e by the Newton inversion (:10597-10606).
+template <int NS, bool KCF>
+struct Rok4Flow {
+  const DevCtx &c;
+  __device__ __forceinline__ void rhs(const double *y, double T_iter, double *out) const {
+    krylov_rhs<NS, KCF>(c, y, T_iter, out);
+  }
+  __device__ __forceinline__ void accept(const double *VEC, double, double &T_iter, double &) const {
+    double rho = VEC[0];
+    for (int n = 1; n < NS; n++) rho = rho + VEC[n];
+    double ri = 1.0 / rho, Y[NS];
+#pragma unroll
+    for (int n = 0; n < NS; n++) Y[n] = VEC[n] * ri;
+    double uu = VEC[NS] * ri, vv = VEC[NS + 1] * ri, ww = VEC[NS + 2] * ri;
+    double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+    double ee = VEC[NS + 3] * ri - qq;
+    T_iter = temp_from_e<NS>(c.t, c.p, ee, T_iter, Y);
+  }
+  __device__ __forceinline__ void done(double, double, int) const {}
+};
+
+// The adiabatic constant-pressure 0-D reactor (no counterpart in the reference,
+// whose batch reactor is constant-volume): state Y_k, clipped at 0 where
+// evaluated; h and p fixed; T from h by the Newton iteration of
+// get_mixture_temperature_from_h_roe_dev (kernels_gpu.F90:6810-6900);
+// rho = p / (R T); dY_k/dt = W_k omega_k / rho.  Per-thread shared-memory rows
+// as in krylov_rhs (launch with STX_CHEM_BLOCK threads).
+template <int NS>
+__device__ __noinline__ void cp_rhs(const DevCtx &c, const double *y, double T_iter, double h, double p,
+                                    double *out) {
+  const DevTab &t = c.t;
+  double Yc[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) Yc[k] = y[k] > 0.0 ? y[k] : 0.0;
+  double tt = temp_from_poly<NS>(t, t.cp, c.p, h, T_iter, Yc);
+  double rm = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) rm = rm + ldg(t.rgas + k) * Yc[k];
+  double rho = p / (rm * tt);
+  __shared__ double s_conc[NS * STX_CHEM_BLOCK], s_rhs[NS * STX_CHEM_BLOCK];
+  double *cs = s_conc + threadIdx.x, *rs = s_rhs + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    cs[k * STX_CHEM_BLOCK] = rho * Yc[k] / ldg(t.mw + k);
+    rs[k * STX_CHEM_BLOCK] = 0.0;
+  }
+  chem_source_sp<NS, STX_CHEM_BLOCK>(t, tt, cs, rs);
+#pragma unroll
+  for (int k = 0; k < NS; k++) out[k] = rs[k * STX_CHEM_BLOCK] / rho;
+}
+
+template <int NS>
+struct Rok4ConstP {
+  const DevCtx &c;
+  double h, p, T0, ign_factor, end_factor;
+  double t_ign, time_reached, T_final;
+  int steps;
+  __device__ __forceinline__ void rhs(const double *y, double T_iter, double *out) const {
+    cp_rhs<NS>(c, y, T_iter, h, p, out);
+  }
+  __device__ __forceinline__ void accept(const double *y, double time, double &T_iter, double &time_end) {
+    double Yc[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) Yc[k] = y[k] > 0.0 ? y[k] : 0.0;
+    T_iter = temp_from_poly<NS>(c.t, c.t.cp, c.p, h, T_iter, Yc);
+    if (t_ign < 0.0 && T_iter > ign_factor * T0) {
+      t_ign = time;
+      double te = end_factor * time;
+      if (te < time_end) time_end = te;
+    }
+  }
+  __device__ __forceinline__ void done(double time, double T_iter, int it) {
+    time_reached = time;
+    T_final = T_iter;
+    steps = it;
+  }
+};
+
+// One ROK4 flow cell.
+template <int NS, bool KCF = false>
+__device__ __forceinline__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const double *fls, double dttry,
+                                          double time_start, double time_end, int simpler) {
+  Rok4Flow<NS, KCF> f{c};
+  rok4_core<NS + 4>(c, f, VEC, T_iter, fls, dttry, time_start, time_end, simpler);
 }
 
 // claim the next cell: warp-aggregated atomicAdd over the currently active lanes

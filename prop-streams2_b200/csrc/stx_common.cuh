@@ -12,6 +12,8 @@
 
 #define STX_MMAX 4     // Krylov dimension M_max (index_define.h:27)
 #define STX_NSTAGE 4   // ROK4 stages (index_define.h:4)
+#define STX_SPR 6      // most reactant (or product) species of one reaction
+#define STX_SPW (4 * STX_SPR)   // sparse row: reactants, products, union (2 STX_SPR)
 
 // species counts compiled into the library
 #define STX_FOR_NS(X) X(9) X(11) X(13) X(14)
@@ -28,6 +30,13 @@ struct DevTab {
   const double *arr_a, *arr_b, *arr_ea, *falloff;   // (nr,2) / (nr,5)
   const double *tb_eff, *r_coeffs, *p_coeffs;       // (nr, ns)
   const double *kc_r;             // repacked [it][lr]
+  // sparse stoichiometry, per reaction lr (built from r_coeffs / p_coeffs):
+  // sp_cnt = nR | nP << 8 | nU << 16; sp_idx / sp_coef [lr][STX_SPW] hold the
+  // reactant species (nu' != 0), the product species (nu'' != 0) and their
+  // union, each in ascending species order, with nu', nu'' and nu'' - nu'.
+  const int *sp_cnt;
+  const unsigned char *sp_idx;
+  const double *sp_coef;
   const double *wk_a, *wk_b;      // Wilke pair factors [l][m]
   int n_eoi;
   const double *aw_eoi, *coeff_eoi, *beta0;
@@ -124,9 +133,20 @@ __device__ double mix_cp(const DevTab &t, double tt, const double *Y) {
   return cploc;
 }
 
-// get_mixture_temperature_from_e_dev (kernels_gpu.F90:6532-6622)
+// get_mixture_temperature_from_e_dev (kernels_gpu.F90:6532-6622) with coef = the
+// cv table; with the cp table it is get_mixture_temperature_from_h_roe_dev
+// (:6810-6900), T from the mixture enthalpy.
 template <int NS>
-__device__ double temp_from_e(const DevTab &t, const DevPar &p, double ee, double T_start, const double *Y) {
+__device__ double temp_from_poly(const DevTab &t, const double *coef, const DevPar &p, double ee, double T_start,
+                                 const double *Y);
+template <int NS>
+__device__ __forceinline__ double temp_from_e(const DevTab &t, const DevPar &p, double ee, double T_start,
+                                              const double *Y) {
+  return temp_from_poly<NS>(t, t.cv, p, ee, T_start, Y);
+}
+template <int NS>
+__device__ double temp_from_poly(const DevTab &t, const double *coef, const DevPar &p, double ee, double T_start,
+                                 const double *Y) {
   int nrange[NS];
 #pragma unroll
   for (int k = 0; k < NS; k++) nrange[k] = 1;
@@ -149,7 +169,7 @@ __device__ double temp_from_e(const DevTab &t, const DevPar &p, double ee, doubl
     }
     double sumb = 0.0;
 #pragma unroll
-    for (int k = 0; k < NS; k++) sumb = sumb + cpc(t, t.cv, t.icr + 1, k + 1, nrange[k]) * Y[k];
+    for (int k = 0; k < NS; k++) sumb = sumb + cpc(t, coef, t.icr + 1, k + 1, nrange[k]) * Y[k];
     double ebar = ee - sumb;
     double den = 0.0, num = 0.0;
     for (int l = t.icl; l <= t.icr; l++) {
@@ -163,7 +183,7 @@ __device__ double temp_from_e(const DevTab &t, const DevPar &p, double ee, doubl
       }
       double cv_l = 0.0;
 #pragma unroll
-      for (int k = 0; k < NS; k++) cv_l = cv_l + cpc(t, t.cv, l, k + 1, nrange[k]) * Y[k];
+      for (int k = 0; k < NS; k++) cv_l = cv_l + cpc(t, coef, l, k + 1, nrange[k]) * Y[k];
       num = num + cv_l * tnum;
       den = den + cv_l * tden;
     }

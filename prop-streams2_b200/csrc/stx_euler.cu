@@ -6,9 +6,9 @@
 //  * x sweep: one CTA of 128 threads per pencil segment; thread t computes face
 //    f0+t, the faces go through shared memory and threads 1..127 apply
 //    fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- no fhat round trip through HBM.
-//  * y/z sweeps: threads along the contiguous i index (coalesced), each thread
-//    marches a chunk of faces along the sweep keeping the previous face flux
-//    in registers; one redundant face per chunk.
+//  * y/z sweeps: tiles of 32 contiguous i (coalesced) x 8 faces along the
+//    sweep, one face per thread, differenced through shared memory; one
+//    redundant face per 7 cells.
 //  * WENO faces use the structure of the multi-species eigenvectors
 //    (kernels_gpu.F90:2703-2984): the species block of L is identity + rank one,
 //    so every characteristic variable follows from two per-point scalars
@@ -143,6 +143,8 @@ __device__ __forceinline__ double weno_rec(const double *vp, const double *vm, i
 }
 
 #define WMAX 8   // 2 * max weno_scheme
+#define CF_LMAX 4                            // largest ep_order / 2 (coeff_deriv1 is 4 x 4)
+#define CF_NPAIR (CF_LMAX * (CF_LMAX + 1) / 2)   // stencil pairs (l, m), m < l <= CF_LMAX
 
 // Central KEEP(n) face flux (kernels_gpu.F90:145-337 and the y/z copies).
 template <int NS, int DIR>
@@ -153,16 +155,24 @@ __device__ __forceinline__ void central_flux(const DevCtx &c, const double *__re
   const int Jn = J_U + DIR;
   int lmax = c.p.ep_order / 2;
   if (lmax < 1) lmax = 1;
+  if (lmax > CF_LMAX) lmax = CF_LMAX;
   const int nkeep = c.p.nkeep;
-#pragma unroll 1
-  for (int lsp = 1; lsp <= NS; lsp++) {
-    double ft1 = 0.0;
-    for (int l = 1; l <= lmax; l++) {
-      double uvs1 = 0.0;
-      for (int m = 0; m <= l - 1; m++) {
+  // Per stencil pair (l, m), a = p - m st, b = p + (l - m) st: the mass-flux
+  // factor (un_a + un_b) (rho_a + rho_b) drhof that the species and the
+  // momentum/energy fluxes share.  The reference forms it inside its species
+  // loop (the KEEP density factor drhof depends on rho_a, rho_b only); it is
+  // formed once per pair here, with the same operations.
+  double up[CF_NPAIR];
+#pragma unroll
+  for (int l = 1; l <= CF_LMAX; l++)
+#pragma unroll
+    for (int m = 0; m < l; m++) {
+      const int q = l * (l - 1) / 2 + m;
+      up[q] = 0.0;
+      if (l <= lmax) {
         long long a = p - m * st, b = p + (l - m) * st;
-        double rhoi = FG(wa, a, J_R), uui = FG(wa, a, Jn), yyi = FG(wa, a, lsp);
-        double rhoip = FG(wa, b, J_R), uuip = FG(wa, b, Jn), yyip = FG(wa, b, lsp);
+        double rhoi = FG(wa, a, J_R), uni = FG(wa, a, Jn);
+        double rhoip = FG(wa, b, J_R), unip = FG(wa, b, Jn);
         double rhom = rhoi + rhoip, drhof;
         if (nkeep <= 0) {
           drhof = 1.0;
@@ -173,18 +183,35 @@ __device__ __forceinline__ void central_flux(const DevCtx &c, const double *__re
           for (int n = 2; n <= nkeep; n++) { int n2 = 2 * n; t = t2 * t; sumden = sumden + t / (1.0 + n2); }
           drhof = 1.0 / sumden;
         }
-        double uv_part = (uui + uuip) * rhom * drhof;
-        uvs1 = uvs1 + uv_part * (yyi + yyip);
+        up[q] = (uni + unip) * rhom * drhof;
       }
-      ft1 = ft1 + c.p.cd1[l][lmax] * uvs1;
+    }
+#pragma unroll 1
+  for (int lsp = 1; lsp <= NS; lsp++) {
+    double ft1 = 0.0;
+#pragma unroll
+    for (int l = 1; l <= CF_LMAX; l++) {
+      if (l <= lmax) {
+        double uvs1 = 0.0;
+#pragma unroll
+        for (int m = 0; m < l; m++) {
+          long long a = p - m * st, b = p + (l - m) * st;
+          uvs1 = uvs1 + up[l * (l - 1) / 2 + m] * (FG(wa, a, lsp) + FG(wa, b, lsp));
+        }
+        ft1 = ft1 + c.p.cd1[l][lmax] * uvs1;
+      }
     }
     double fh1 = 0.25 * ft1;
     fh[lsp - 1] = fz ? 0.0 : fh1;
   }
   double ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
-  for (int l = 1; l <= lmax; l++) {
+#pragma unroll
+  for (int l = 1; l <= CF_LMAX; l++) {
+    if (l > lmax) break;
     double uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs6 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0;
-    for (int m = 0; m <= l - 1; m++) {
+#pragma unroll
+    for (int m = 0; m < l; m++) {
+      const int q = l * (l - 1) / 2 + m;
       long long a = p - m * st, b = p + (l - m) * st;
       double rhoi = FG(wa, a, J_R), uui = FG(wa, a, J_U), vvi = FG(wa, a, J_V), wwi = FG(wa, a, J_W);
       double enti = FG(wa, a, J_H), ppi = FG(wa, a, J_P);
@@ -192,30 +219,26 @@ __device__ __forceinline__ void central_flux(const DevCtx &c, const double *__re
       double entip = FG(wa, b, J_H), ppip = FG(wa, b, J_P);
       double uni = DIR == 0 ? uui : (DIR == 1 ? vvi : wwi);
       double unip = DIR == 0 ? uuip : (DIR == 1 ? vvip : wwip);
-      double rhom = rhoi + rhoip;
+      double uv_part = up[q];
       if (nkeep >= 0) {
         double eei = enti - ppi / rhoi - 0.5 * (uui * uui + vvi * vvi + wwi * wwi);
         double eeip = entip - ppip / rhoip - 0.5 * (uuip * uuip + vvip * vvip + wwip * wwip);
-        double eem = eei + eeip, drhof, deef;
+        double eem = eei + eeip, deef;
         if (nkeep == 0) {
-          drhof = 1.0; deef = 1.0;
+          deef = 1.0;
         } else {
-          double drho = 2.0 * (rhoip - rhoi) / rhom;
           double dee = 2.0 * (eeip - eei) / eem;
-          double tr = (0.5 * drho) * (0.5 * drho), te = (0.5 * dee) * (0.5 * dee);
-          double tr2 = tr, te2 = te;
-          double sdr = 1.0 + tr / 3.0, sde = 1.0 + te, sne = 1.0 + te / 3.0;
+          double te = (0.5 * dee) * (0.5 * dee);
+          double te2 = te;
+          double sde = 1.0 + te, sne = 1.0 + te / 3.0;
           for (int n = 2; n <= nkeep; n++) {
             int n2 = 2 * n;
-            tr = tr2 * tr; te = te2 * te;
-            sdr = sdr + tr / (1.0 + n2);
+            te = te2 * te;
             sde = sde + te;
             sne = sne + te / (1.0 + n2);
           }
-          drhof = 1.0 / sdr;
           deef = sne / sde;
         }
-        double uv_part = (uni + unip) * rhom * drhof;
         uvs2 = uvs2 + uv_part * (uui + uuip);
         uvs3 = uvs3 + uv_part * (vvi + vvip);
         uvs4 = uvs4 + uv_part * (wwi + wwip);
@@ -224,7 +247,6 @@ __device__ __forceinline__ void central_flux(const DevCtx &c, const double *__re
         uvs5_p = uvs5_p + 4.0 * (uni * ppip + unip * ppi);
         uvs6 = uvs6 + (2.0) * (ppi + ppip);
       } else {
-        double uv_part = (uni + unip) * rhom;
         uvs2 = uvs2 + uv_part * (uui + uuip);
         uvs3 = uvs3 + uv_part * (vvi + vvip);
         uvs4 = uvs4 + uv_part * (wwi + wwip);
@@ -517,26 +539,33 @@ __device__ __forceinline__ void face_flux(const DevCtx &c, const double *__restr
   }
 }
 
-// x sweep: faces through shared memory
+// x sweep: the faces nmin-1..nmax of every (j, k) row are numbered as one
+// sequence F = row * nf + (f - nmin + 1); CTA b computes faces 127 b .. 127 b + 127
+// (one face shared with the next CTA), puts them in shared memory, and the
+// threads whose face is not the first of its row form
+// fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- every thread busy for any nx.
 template <int NS>
-__global__ void __launch_bounds__(128) k_euler_x(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl,
-                                                 int nmin, int nmax, int overwrite) {
+__global__ void __launch_bounds__(128, 4) k_euler_x(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl,
+                                                    int nmin, int nmax, int overwrite) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
   __shared__ double sf[NV][128];
-  int j = blockIdx.y + 1, k = blockIdx.z + 1;
-  int f0 = nmin - 1 + blockIdx.x * 127;
-  int f = f0 + threadIdx.x;
-  double fh[NV];
-  if (f <= nmax) {
+  const long long nf = nmax - nmin + 2;
+  const long long F = (long long)blockIdx.x * 127 + threadIdx.x;
+  const bool act = F < nf * g.ny * g.nz;
+  const long long row = F / nf;
+  const int f = nmin - 1 + (int)(F - row * nf);
+  const int j = 1 + (int)(row % g.ny), k = 1 + (int)(row / g.ny);
+  if (act) {
+    double fh[NV];
     long long p = gidx(g, f, j, k);
     face_flux<NS, 0>(c, wa, p, 1, f, g.nx, fh);
 #pragma unroll
     for (int m = 0; m < NV; m++) sf[m][threadIdx.x] = fh[m];
   }
   __syncthreads();
-  int i = f;
-  if (threadIdx.x >= 1 && i <= nmax) {
+  if (threadIdx.x >= 1 && act && f >= nmin) {
+    const int i = f;
     long long q = fidx(g, i, j, k);
     double met = ldg(g.dcsidx + i - 1);
 #pragma unroll
@@ -547,36 +576,41 @@ __global__ void __launch_bounds__(128) k_euler_x(DevCtx c, const double *__restr
   }
 }
 
-// y / z sweeps: march along the sweep
+// y / z sweeps: a CTA is a tile of YZ_TI consecutive i (one warp, coalesced)
+// by YZ_TF consecutive faces of the sweep; every thread computes one face, the
+// faces go through shared memory, and rows 1..YZ_TF-1 form the YZ_TF-1 cells
+// fl(f) += (fhat_f - fhat_{f-1}) * d(eta)/dy.  One redundant face per tile.
+#define YZ_TI 32
+#define YZ_TF 8
 template <int NS, int DIR>
-__global__ void __launch_bounds__(128) k_euler_yz(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl,
-                                                  int nmin, int nmax, int chunk, int overwrite) {
+__global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const double *__restrict__ wa,
+                                                           double *__restrict__ fl, int nmin, int nmax, int overwrite) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
-  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (i > g.nx) return;
+  __shared__ double sf[NV][YZ_TF][YZ_TI];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  int i = blockIdx.x * YZ_TI + tx + 1;
   int tr = blockIdx.y + 1;                 // k for the y sweep, j for the z sweep
-  int c0 = nmin + blockIdx.z * chunk;
-  int c1 = min(c0 + chunk - 1, nmax);
+  int f = nmin - 1 + blockIdx.z * (YZ_TF - 1) + ty;
   long long st = DIR == 1 ? (long long)g.nxg : (long long)g.nxg * g.nyg;
-  const double *met = DIR == 1 ? g.detady : g.dzitdz;
   int nsw = DIR == 1 ? g.ny : g.nz;
-  double prev[NV], cur[NV];
-  {
-    int f = c0 - 1;
+  bool act = i <= g.nx && f <= nmax;
+  if (act) {
+    double fh[NV];
     long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
-    face_flux<NS, DIR>(c, wa, p, st, f, nsw, prev);
+    face_flux<NS, DIR>(c, wa, p, st, f, nsw, fh);
+#pragma unroll
+    for (int m = 0; m < NV; m++) sf[m][ty][tx] = fh[m];
   }
-  for (int f = c0; f <= c1; f++) {
-    long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
-    face_flux<NS, DIR>(c, wa, p, st, f, nsw, cur);
+  __syncthreads();
+  if (ty >= 1 && act) {
+    const double *met = DIR == 1 ? g.detady : g.dzitdz;
     long long q = DIR == 1 ? fidx(g, i, f, tr) : fidx(g, i, tr, f);
     double mt = ldg(met + f - 1);
 #pragma unroll
     for (int m = 0; m < NV; m++) {
-      double d = (cur[m] - prev[m]) * mt;
+      double d = (sf[m][ty][tx] - sf[m][ty - 1][tx]) * mt;
       FI(fl, q, m + 1) = overwrite ? d : FI(fl, q, m + 1) + d;
-      prev[m] = cur[m];
     }
   }
 }
@@ -587,15 +621,16 @@ static int euler_t(const DevCtx &c, cudaStream_t s, int dir, const double *wa, d
   if (nmax - nmin < 0) return STX_OK;
   if (2 * c.p.weno_scheme > WMAX) return STX_E_UNSUPPORTED;
   if (dir == 0) {
-    int ncell = nmax - nmin + 1;
-    dim3 grid((ncell + 126) / 127, g.ny, g.nz);
-    k_euler_x<NS><<<grid, 128, 0, s>>>(c, wa, fl, nmin, nmax, ow);
+    long long nface = (long long)(nmax - nmin + 2) * g.ny * g.nz;
+    long long nb = (nface - 1 + 126) / 127;     // CTA b covers faces 127 b .. 127 b + 127
+    if (nb > 0x7fffffffLL) return STX_E_INVALID;
+    k_euler_x<NS><<<(unsigned)nb, 128, 0, s>>>(c, wa, fl, nmin, nmax, ow);
   } else {
-    int chunk = 16;
     int ncell = nmax - nmin + 1;
-    dim3 grid((g.nx + 127) / 128, dir == 1 ? g.nz : g.ny, (ncell + chunk - 1) / chunk);
-    if (dir == 1) k_euler_yz<NS, 1><<<grid, 128, 0, s>>>(c, wa, fl, nmin, nmax, chunk, ow);
-    else k_euler_yz<NS, 2><<<grid, 128, 0, s>>>(c, wa, fl, nmin, nmax, chunk, ow);
+    dim3 grid((g.nx + YZ_TI - 1) / YZ_TI, dir == 1 ? g.nz : g.ny, (ncell + YZ_TF - 2) / (YZ_TF - 1));
+    dim3 block(YZ_TI, YZ_TF);
+    if (dir == 1) k_euler_yz<NS, 1><<<grid, block, 0, s>>>(c, wa, fl, nmin, nmax, ow);
+    else k_euler_yz<NS, 2><<<grid, block, 0, s>>>(c, wa, fl, nmin, nmax, ow);
   }
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;

@@ -23,3 +23,6 @@ int launch_rok4(const DevCtx &c, cudaStream_t s, double *w, const double *wa, co
 int launch_rosenbrock(const DevCtx &c, cudaStream_t s, double *w, double *wa, double dttry, double t0, double t1,
                       unsigned int *counter);
 int launch_chem_explicit(const DevCtx &c, cudaStream_t s, double *w, double *wa, double *fl);
+int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
+                   double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
+                   double *t_end, int *nsteps, unsigned int *counter);

@@ -135,6 +135,7 @@ ORACLE_SIGNATURES = [
     ("ox_krylov_cell", None, [_VP, _VP, _D, _D, _VP, _D, _D, _D, _I]),
     ("ox_rosenbrock_cell", None, [_VP, _VP, _VP, _VP, _D, _D, _D]),
     ("ox_temperature_from_e", _D, [_VP, _D, _D, _VP]),
+    ("ox_batch0d_cp", None, [_VP, _I, _VP, _VP, _VP, _D, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP]),
 ]
 
 
