@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the baseline")
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer leg (default: --steps)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="turbulence", choices=["turbulence", "reactors"],
+                    help="turbulence: the headline reacting-step benchmark; reactors: batched 0-D reactors")
+    ap.add_argument("--reactors", type=int, default=8192, help="reactors per GPU (--workload reactors)")
+    ap.add_argument("--t-max", type=float, default=1e-2, help="longest integration of a reactor [s]")
+    ap.add_argument("--max-steps", type=int, default=20000, help="ROK4 step cap per reactor")
     return ap.parse_args()
 
 
@@ -319,8 +324,158 @@ def run_stx(args):
     return 0
 
 
+# ------------------------------------------------------------------ batched 0-D reactors
+R_METRIC = "reactor-solves/s"
+
+
+def reactors_config(args, world):
+    return {"workload": f"{args.reactors} adiabatic constant-pressure H2/air 0-D reactors per GPU (9 species, "
+                        f"21 reactions), T0~U(900,1500) K, p~logU(1,40) atm, phi~U(0.3,3), ROK4, each integrated "
+                        f"to min(2 t_ign, {args.t_max:g} s) with t_ign the first T > 1.05 T0, at most "
+                        f"{args.max_steps} steps, one persistent launch, coldest reactors first",
+            "reactors_per_gpu": args.reactors, "species": 9, "reactions": 21, "precision_form": "plain FP64",
+            "parallelism": f"dp{world} (independent reactor sets)",
+            "l2": "compute bound; inputs are a few hundred KB"}
+
+
+def cpu_reactors(args, n_sample):
+    """The oracle's constant-pressure reactors on a bounded sample (solves/s)."""
+    import ctypes as C
+    import numpy as np
+    from stx import configs, native
+    from stx import case as CS
+    from stx import mech as M
+    from stx.reactors import sample_h2air
+    mech = configs.mechanism("h2air_9sp")
+    tb = M.build_tables(mech, 101325.0, 200.0, 5500.0, 1.0)
+    cfg = CS.default_ini(1, 1, 1, L=(1e-3,) * 3, Y=np.full(mech.ns, 1.0 / mech.ns), ns=mech.ns)
+    case = CS.Case(cfg, tb, alloc_fields=False)
+    oracle_so = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.exists(oracle_so):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    lib = native.load_oracle()
+    par, tab, grid = case.params_struct(), case.tables_struct(), case.grid_struct()
+    ctx = lib.ox_ctx_create(C.byref(par), C.byref(tab), C.byref(grid))
+    cores = os.cpu_count() or 1
+    lib.ox_set_threads(cores)
+    T0, p0, Y0 = sample_h2air(n_sample, args.seed, mech)
+    Y0 = np.ascontiguousarray(Y0)
+    Y = np.empty_like(Y0); T = np.empty(n_sample); ti = np.empty(n_sample); te = np.empty(n_sample)
+    ns = np.empty(n_sample, dtype=np.int32)
+    vp = lambda a: C.c_void_p(a.ctypes.data)
+    t0 = time.perf_counter()
+    lib.ox_batch0d_cp(ctx, n_sample, vp(T0), vp(p0), vp(Y0), args.t_max, 1e-8, 1.05, 2.0, args.max_steps, vp(Y),
+                      vp(T), vp(ti), vp(te), vp(ns))
+    el = time.perf_counter() - t0
+    lib.ox_ctx_destroy(ctx)
+    return n_sample / el, cores, f"{n_sample} reactors of the same distribution (seed {args.seed}), {el:.1f} s"
+
+
+def run_reactors(args):
+    import torch
+    import torch.distributed as dist
+    from stx.reactors import BatchReactors, sample_h2air
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    br = BatchReactors("h2air_9sp", device=str(dev))
+    T0, p0, Y0 = sample_h2air(args.reactors, args.seed + rank, br.mech)
+    dT0, dp0, dY0 = (torch.as_tensor(a, dtype=torch.float64, device=dev).contiguous() for a in (T0, p0, Y0))
+
+    def solve():
+        return br.integrate(dT0, dp0, dY0, args.t_max, 1e-8, 1.05, 2.0, args.max_steps, sync=False,
+                            order="coldest_first")
+
+    for _ in range(args.warmup):
+        out = solve()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        out = solve()
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_max = float(ms.item())
+    value = args.reactors * world * args.steps / (ms_max / 1e3)
+    nsteps = out["nsteps"].cpu().numpy()
+    t_ign = out["t_ign"].cpu().numpy()
+    status = br.status()
+
+    # e2e: inputs from pinned host memory, all outputs back to pinned host memory, every step
+    hT0, hp0, hY0 = (torch.as_tensor(a, dtype=torch.float64).contiguous().pin_memory() for a in (T0, p0, Y0))
+    hout = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in out.items()}
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        dT0.copy_(hT0, non_blocking=True); dp0.copy_(hp0, non_blocking=True); dY0.copy_(hY0, non_blocking=True)
+        o = solve()
+        for k in hout:
+            hout[k].copy_(o[k], non_blocking=True)
+    t1.record()
+    torch.cuda.synchronize()
+    ms2 = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms2, op=dist.ReduceOp.MAX)
+    e2e = args.reactors * world * args.steps / (float(ms2.item()) / 1e3)
+    h2d = sum(t.numel() * t.element_size() for t in (hT0, hp0, hY0))
+    d2h = sum(t.numel() * t.element_size() for t in hout.values())
+    line = {"metric": R_METRIC, "value": value, "unit": R_METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": reactors_config(args, world),
+            "reactor_steps_per_s": float(nsteps.sum()) * world * args.steps / (ms_max / 1e3),
+            "steps_per_reactor": {"mean": float(nsteps.mean()), "max": int(nsteps.max()),
+                                  "capped": int((nsteps > args.max_steps).sum())},
+            "ignited": int((t_ign > 0).sum()), "clocks": ck, "gpu_launches": args.steps,
+            "e2e": {"value": e2e, "unit": R_METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "path": "BatchReactors.integrate -> stx_batch0d_integrate, inputs from and outputs to pinned "
+                            "host memory every step"},
+            "status_bits": status}
+    if world == 1 and rank == 0 and not args.no_cpu:
+        rate, cores, sample = cpu_reactors(args, 64)
+        line["cpu_baseline"] = {"value": rate, "unit": R_METRIC, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    br.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "reactors":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) != 0:
+                return 0
+            rate, cores, sample = cpu_reactors(args, 64)
+            print(json.dumps({"impl": "reference", "metric": R_METRIC, "value": rate, "unit": R_METRIC,
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic (seeded)", "config": reactors_config(args, args.gpus),
+                              "cpu_baseline": {"value": rate, "unit": R_METRIC, "cores": cores, "kind": "port",
+                                               "sample": sample},
+                              "e2e": {"value": rate, "unit": R_METRIC, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
+        return run_reactors(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_stx(args)

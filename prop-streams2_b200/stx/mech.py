@@ -613,6 +613,15 @@ def mixture_cp(tb: Tables, T: float, Y: np.ndarray) -> float:
 
 def mixture_e(tb: Tables, T: float, Y: np.ndarray) -> float:
     """``get_e_from_temperature``: sum_k Y_k e_k(T) with e_k from the cv polynomial."""
+    return _mixture_poly_int(tb, tb.cv_coeff, T, Y)
+
+
+def mixture_h(tb: Tables, T: float, Y: np.ndarray) -> float:
+    """sum_k Y_k h_k(T) with h_k from the cp polynomial (get_species_h_from_temperature)."""
+    return _mixture_poly_int(tb, tb.cp_coeff, T, Y)
+
+
+def _mixture_poly_int(tb: Tables, coeff: np.ndarray, T: float, Y: np.ndarray) -> float:
     e = 0.0
     for k in range(tb.ns):
         m = 1
@@ -625,7 +634,7 @@ def mixture_e(tb: Tables, T: float, Y: np.ndarray) -> float:
                 else:
                     ju = jm
             m = min(max(jl, 1), tb.nsetcv)
-        c = tb.cv_coeff[:, k, m - 1]
+        c = coeff[:, k, m - 1]
         ek = c[tb.indx_cp_r + 1 - tb.indx_cp_l]
         for l in range(tb.indx_cp_l, tb.indx_cp_r + 1):
             if l == -1:

@@ -117,6 +117,44 @@ def test_oracle_batch_reactor_matches_reference_output():
     o.close()
 
 
+def test_oracle_constant_pressure_reactor_conserves_h_and_ignites():
+    """The constant-pressure 0-D reactor of the oracle (the checker of
+    stx_batch0d_integrate): h and sum Y_k stay constant through ignition,
+    ignition is detected at T > 1.05 T0 and the run ends at 2 t_ign, and a
+    hotter start ignites earlier."""
+    from stx import configs, native
+    from stx.reactors import sample_h2air
+    mech = configs.mechanism("h2air_9sp")
+    tb = M.build_tables(mech, 101325.0, 200.0, 5500.0, 1.0)
+    cfg = CS.default_ini(1, 1, 1, L=(1e-3,) * 3, Y=np.full(mech.ns, 1.0 / mech.ns), ns=mech.ns)
+    case = CS.Case(cfg, tb, alloc_fields=False)
+    lib = native.load_oracle()
+    par, tab, grid = case.params_struct(), case.tables_struct(), case.grid_struct()
+    ctx = lib.ox_ctx_create(C.byref(par), C.byref(tab), C.byref(grid))
+    lib.ox_set_threads(4)
+    T0 = np.array([1300.0, 1400.0, 1500.0, 1450.0])
+    p0 = np.array([1.0, 1.0, 1.0, 5.0]) * 101325.0
+    Y0 = np.ascontiguousarray(np.stack([configs.h2air_Y(1.0, mech)] * 4, axis=1))
+    n = 4
+    Y = np.empty_like(Y0); T = np.empty(n); ti = np.empty(n); te = np.empty(n); ns = np.empty(n, dtype=np.int32)
+    vp = lambda a: C.c_void_p(a.ctypes.data)
+    lib.ox_batch0d_cp(ctx, n, vp(T0), vp(p0), vp(Y0), 1e-3, 1e-8, 1.05, 2.0, 100000, vp(Y), vp(T), vp(ti), vp(te),
+                      vp(ns))
+    assert lib.ox_status(ctx, 1) & 0x2 == 0
+    lib.ox_ctx_destroy(ctx)
+    assert np.all(ti > 0) and np.allclose(te, 2.0 * ti, rtol=1e-12)
+    assert ti[0] > ti[1] > ti[2]
+    assert np.max(np.abs(Y.sum(axis=0) - 1.0)) < 1e-12
+    for r in range(n):
+        h0 = M.mixture_h(tb, T0[r], Y0[:, r])
+        assert abs(M.mixture_h(tb, T[r], np.maximum(Y[:, r], 0.0)) - h0) < 1e-9 * abs(h0) + 1e-6
+        assert T[r] > 2000.0                        # burnt (at 2 t_ign, near but below T_ad)
+    # the sampler of the batched workload is seeded and in range
+    a, b, c = sample_h2air(16, 3, mech)
+    assert np.all((a >= 900) & (a <= 1500)) and np.all((b >= 101325.0) & (b <= 40 * 101325.0 + 1e-6))
+    assert np.allclose(c.sum(axis=0), 1.0)
+
+
 def _declared_symbols():
     hdr = open(os.path.join(H.REPO, "include", "stx.h")).read()
     return sorted(set(re.findall(r"\b(stx_[a-z0-9_]+)\s*\(", hdr)))
@@ -133,6 +171,15 @@ def test_libstx_exports_every_declared_symbol():
     lib = C.CDLL(so)          # loads without a GPU (cudart is linked statically)
     lib.stx_abi_version.restype = C.c_int
     assert lib.stx_abi_version() == 1
+
+
+def test_every_declared_entry_point_has_a_python_binding():
+    """Every stx_* function of include/stx.h carries a ctypes signature in
+    stx/native.py (the allocation-free entry point is bound by its own test)."""
+    from stx import native
+    have = {s[0] for s in native.STX_SIGNATURES} | {"stx_rosenbrock_krylov_noalloc"}
+    missing = [s for s in _declared_symbols() if s not in have]
+    assert not missing, missing
 
 
 def test_ctx_create_rejects_unsupported_options_without_touching_the_gpu():

@@ -1,0 +1,90 @@
+"""Batched constant-pressure 0-D reactors (stx_batch0d_integrate) against the
+oracle's ox_batch0d_cp on the same seeded reactors.
+
+An adaptive integration through ignition is sensitive to last-bit changes (CUDA
+and libm exp/pow differ by an ulp): the oracle itself moves its ignition times
+by up to ~5e-4 relative (median 2e-7) when T0 is perturbed by one ulp.  The
+bar is therefore: ignition times within 1e-3 relative everywhere and 1e-5 in
+the median; final temperatures within 1e-3 relative; the major species
+(Y > 1e-3) within 1e-3 relative.  A reactor's result does not depend on the
+other reactors of the batch (bit-identical alone and in the batch)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import helpers as H  # noqa: F401  (puts the package on sys.path)
+
+pytestmark = pytest.mark.gpu
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from stx import native  # noqa: E402
+from stx import mech as M  # noqa: E402
+from stx.reactors import BatchReactors, sample_h2air  # noqa: E402
+
+T_MAX, DTTRY, MAXSTEPS = 5e-3, 1e-8, 60000
+
+
+@pytest.fixture(scope="module")
+def batch():
+    br = BatchReactors("h2air_9sp")
+    yield br
+    br.close()
+
+
+def oracle_run(br, T0, p0, Y0):
+    lib = native.load_oracle()
+    par, tab, grid = br.case.params_struct(), br.case.tables_struct(), br.case.grid_struct()
+    ctx = lib.ox_ctx_create(C.byref(par), C.byref(tab), C.byref(grid))
+    lib.ox_set_threads(8)
+    n = T0.size
+    Y0 = np.ascontiguousarray(Y0)
+    Y = np.empty_like(Y0); T = np.empty(n); ti = np.empty(n); te = np.empty(n); ns = np.empty(n, dtype=np.int32)
+    vp = lambda a: C.c_void_p(a.ctypes.data)
+    lib.ox_batch0d_cp(ctx, n, vp(T0), vp(p0), vp(Y0), T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS, vp(Y), vp(T), vp(ti), vp(te),
+                      vp(ns))
+    lib.ox_ctx_destroy(ctx)
+    return dict(Y=Y, T=T, t_ign=ti, t_end=te, nsteps=ns)
+
+
+def test_batch_reactors_match_oracle(batch):
+    T0, p0, Y0 = sample_h2air(96, 21, batch.mech, T_range=(1050.0, 1500.0))
+    o = oracle_run(batch, T0, p0, Y0)
+    g = {k: v.cpu().numpy() for k, v in batch.integrate(T0, p0, Y0, T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS).items()}
+    ign = o["t_ign"] > 0
+    assert ign.sum() >= 80
+    assert np.array_equal(g["t_ign"] > 0, ign)
+    r = np.abs(g["t_ign"][ign] - o["t_ign"][ign]) / o["t_ign"][ign]
+    assert r.max() < 1e-3 and np.median(r) < 1e-5, (r.max(), np.median(r))
+    assert np.max(np.abs(g["T"] - o["T"]) / o["T"]) < 1e-3
+    big = o["Y"] > 1e-3
+    assert np.max(np.abs(g["Y"] - o["Y"])[big] / o["Y"][big]) < 1e-3
+    # the adaptive step sequences agree almost everywhere
+    assert np.median(np.abs(g["nsteps"] - o["nsteps"])) <= 2
+
+
+def test_batch_reactor_alone_equals_in_batch(batch):
+    T0, p0, Y0 = sample_h2air(64, 5, batch.mech, T_range=(1100.0, 1500.0))
+    full = batch.integrate(T0, p0, Y0, T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS)
+    cold = batch.integrate(T0, p0, Y0, T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS, order="coldest_first")
+    for k in full:
+        assert torch.equal(full[k], cold[k]), k
+    for r in (0, 17, 63):
+        one = batch.integrate(T0[r:r + 1], p0[r:r + 1], Y0[:, r:r + 1], T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS)
+        for k in ("Y", "T", "t_ign", "t_end", "nsteps"):
+            a = full[k][..., r].cpu().numpy()
+            b = one[k][..., 0].cpu().numpy()
+            assert np.array_equal(a, b), (k, r)
+
+
+def test_batch_reactor_conserves_enthalpy_and_mass(batch):
+    T0, p0, Y0 = sample_h2air(32, 9, batch.mech, T_range=(1200.0, 1500.0))
+    g = {k: v.cpu().numpy() for k, v in batch.integrate(T0, p0, Y0, T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS).items()}
+    assert np.max(np.abs(g["Y"].sum(axis=0) - 1.0)) < 1e-12
+    tb = batch.case.tb
+    h0 = np.array([M.mixture_h(tb, T0[r], Y0[:, r]) for r in range(T0.size)])
+    h1 = np.array([M.mixture_h(tb, g["T"][r], np.maximum(g["Y"][:, r], 0.0)) for r in range(T0.size)])
+    assert np.max(np.abs(h1 - h0) / np.abs(h0).max()) < 1e-9
+    assert np.all(g["T"] > 2000.0)
