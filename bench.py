@@ -48,8 +48,15 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the baseline")
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer leg (default: --steps)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="turbulence", choices=["turbulence", "reactors"],
-                    help="turbulence: the headline reacting-step benchmark; reactors: batched 0-D reactors")
+    ap.add_argument("--workload", default="turbulence", choices=["turbulence", "reactors", "flame", "serve"],
+                    help="turbulence: the headline reacting-step benchmark; reactors: batched 0-D reactors; "
+                         "flame: the 2000-cell 1-D premixed flame of the reference's published timing; "
+                         "serve: a Poisson stream of mixed 0-D / 1-D / 2-D solves")
+    ap.add_argument("--graph-steps", type=int, default=10, help="steps per captured graph (--workload flame)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="fp64: the reference method; mixed: FP32 face fluxes and transport, FP64 residual/chemistry")
+    ap.add_argument("--requests", type=int, default=2000, help="requests of the served mix (--workload serve)")
+    ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate [1/s] (--workload serve)")
     ap.add_argument("--reactors", type=int, default=8192, help="reactors per GPU (--workload reactors)")
     ap.add_argument("--t-max", type=float, default=1e-2, help="longest integration of a reactor [s]")
     ap.add_argument("--max-steps", type=int, default=20000, help="ROK4 step cap per reactor")
@@ -176,6 +183,32 @@ def run_reference(args):
 KNAMES = ["eval_aux", "ducros", "ghost", "euler", "visc", "rk", "chem", "dt"]
 
 
+def mixed_error(dev, seed, n=48, steps=5):
+    """Max relative error in T and Y_k (Y_k > 1e-8) of the mixed form against the
+    FP64 form after `steps` reacting steps on an n^3 same-resolution sample."""
+    import numpy as np
+    import torch
+    from stx import configs
+    from stx.solver import Solver
+    case = configs.turbulence_case(n)
+    out = {}
+    for form in ("fp64", "mixed"):
+        W, WA = configs.turbulence_fields(case, seed, xp=torch, device=dev)
+        s = Solver(case, device=str(dev), w=W, w_aux=WA)
+        s.set_precision(form)
+        s.prepare()
+        for _ in range(steps):
+            s.step()
+        torch.cuda.synchronize()
+        out[form] = (case.interior(s.w_aux[case.J("T")]).cpu().numpy(), case.interior(s.w_aux[:case.ns]).cpu().numpy())
+        s.close()
+    (T0, Y0), (T1, Y1) = out["fp64"], out["mixed"]
+    big = Y0 > 1e-8
+    return {"T_rel_max": float(np.max(np.abs(T1 - T0) / T0)),
+            "Y_rel_max": float(np.max(np.abs(Y1 - Y0)[big] / Y0[big])),
+            "sample": f"{n}^3 cells, {steps} steps, GPU FP64 form (= oracle to 1e-8) vs mixed form"}
+
+
 def run_stx(args):
     import ctypes as C
     import numpy as np
@@ -199,6 +232,8 @@ def run_stx(args):
     sol = Solver(case, device=str(dev), w=W, w_aux=WA)
     del W, WA
     lib = sol.lib
+    if args.precision == "mixed":
+        sol.set_precision("mixed")
 
     from stx import dist as D
 
@@ -305,13 +340,19 @@ def run_stx(args):
 
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": config_dict(n, world, {"dt_last": sol.dt}),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
+            "data": "synthetic (seeded)",
+            "config": config_dict(n, world, {"dt_last": sol.dt,
+                                             "precision_form": "plain FP64" if args.precision == "fp64" else
+                                             "mixed: FP32 central/viscous face fluxes and transport properties, "
+                                             "FP64 RK residual, Newton T(e), WENO faces and chemistry"}),
             "roofline": roofline, "clocks": ck, "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": wbytes, "d2h_bytes_per_step": wbytes,
                     "path": "stx_advance_solution et al. through the C ABI, state w copied from pinned host memory "
                             "before and back after every step"},
             "kernels": cls, "status_bits": status}
+    if args.precision == "mixed" and rank == 0:
+        line["error_vs_fp64"] = mixed_error(dev, args.seed)
     if world == 1 and rank == 0 and not args.no_cpu:
         rate, cores, sample = cpu_run(args.cpu_n, args.cpu_budget, args.seed)
         line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample}
@@ -459,8 +500,197 @@ def run_reactors(args):
     return 0
 
 
+# ------------------------------------------------------------------ 1-D premixed flame
+# The reference's one published timing (examples/laminar_premix_flame/data.dat:132):
+# 7.0269314 ms per RK step for 2000 cells on one A100 (sm_80), i.e. 2.846e5 cell-steps/s.
+FLAME_PUBLISHED = 2000.0 / 7.0269314e-3
+
+
+def flame_config(world, graph_steps):
+    return {"workload": "1-D laminar premixed H2/air flame, 2000 cells over 0.03 m, 11 species / 21 reactions "
+                        "(examples/laminar_premix_flame settings: inflow xmin, extrapolation xmax, WENO5-Z on every "
+                        "face + KEEP(2), simpler splitting, ROK4, Wray RK3, fixed dt 1e-8 s); synthetic tanh flame "
+                        "(phi 0.6, 298 K -> 1847 K) standing in for premix.dat",
+            "cells_per_gpu": 2000, "species": 11, "reactions": 21, "precision_form": "plain FP64",
+            "parallelism": f"dp{world} (independent flames)",
+            "launch": f"{graph_steps} steps per CUDA graph launch",
+            "published_baseline": "7.0269314 ms/step on one A100 (data.dat:132) = 2.846e5 cell-steps/s",
+            "l2": "fields (12 MB) fit in L2; latency bound"}
+
+
+def cpu_flame(args, budget_s=20.0):
+    """The oracle on the same flame, all host cores, for about budget_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    oracle_so = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.exists(oracle_so):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    from stx import configs
+    from driver import OracleSolver
+    cores = os.cpu_count() or 1
+    o = OracleSolver(configs.flame_case(2000, phi=0.6, Tu=298.0), threads=cores)
+    o.prepare()
+    o.step()
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        o.step()
+        k += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or k >= 2000:
+            break
+    o.close()
+    return 2000 * k / el, cores, f"the same 2000-cell flame, {k} steps after 1 warm-up, {el:.1f} s"
+
+
+def run_flame(args):
+    import torch
+    import torch.distributed as dist
+    from stx import configs
+    from stx.solver import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    case = configs.flame_case(2000, phi=0.6, Tu=298.0)
+    sol = Solver(case, device=str(dev))
+    sol.prepare()
+    G = max(1, args.graph_steps)
+    K = max(G, (args.steps // G) * G)
+    g = sol.capture(G)
+    for _ in range(max(1, args.warmup // G + (args.warmup % G > 0))):
+        sol.replay(g)
+    torch.cuda.synchronize()
+    check_lib = sol.lib
+    check_lib.stx_profile_enable(sol.ctx, 0)
+    clocks = Clocks(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K // G):
+        sol.replay(g)
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_max = float(ms.item())
+    value = 2000 * world * K / (ms_max / 1e3)
+    status = sol.status()
+    # e2e: step by step through the C ABI, the state from pinned host memory before and back after every step
+    host_w = torch.empty(sol.w.shape, dtype=torch.float64, pin_memory=True)
+    host_w.copy_(sol.w)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    K2 = min(K, 200)
+    t0.record()
+    for _ in range(K2):
+        sol.w.copy_(host_w, non_blocking=True)
+        sol.step()
+        host_w.copy_(sol.w, non_blocking=True)
+    t1.record()
+    torch.cuda.synchronize()
+    ms2 = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms2, op=dist.ReduceOp.MAX)
+    e2e = 2000 * world * K2 / (float(ms2.item()) / 1e3)
+    wbytes = sol.w.numel() * 8
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / (FLAME_PUBLISHED * world), "dtype": "f64", "data": "synthetic (seeded)",
+            "config": flame_config(world, G), "clocks": ck, "gpu_launches": K // G,
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": wbytes, "d2h_bytes_per_step": wbytes,
+                    "path": "Solver.step (stx_compute_aux / stx_advance_solution through the C ABI, ~50 launches "
+                            "per step, no graph), state w from pinned host memory before and back after every step"},
+            "status_bits": status}
+    if world == 1 and rank == 0 and not args.no_cpu:
+        rate, cores, sample = cpu_flame(args)
+        line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------------------------------ served mix
+S_METRIC = "solves/s"
+
+
+def run_serve(args):
+    import torch
+    from stx import configs
+    from stx.serve import Server, mixed_requests
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    srv = Server(device=f"cuda:{local}", max_grid=32, chunk=5)
+    mech = configs.mechanism("h2air_9sp")
+    warm = mixed_requests(max(3, args.warmup * 4), 1e9, args.seed + 97 + rank, mech)
+    srv.run(warm, realtime=False)
+    reqs = mixed_requests(args.requests, args.rate, args.seed + rank, mech)
+    clocks = Clocks(local)
+    clocks.start()
+    stats = srv.run(reqs, realtime=True)
+    ck = clocks.stop()
+    srv.close()
+    cfg = {"workload": f"served stream of {args.requests} requests per GPU, Poisson arrivals at {args.rate:g}/s: "
+                       f"60% 0-D H2/air reactors (the batched-reactor distribution, to min(2 t_ign, 10 ms)), "
+                       f"30% 1-D premixed flames (nx~U{{512..4096}}, phi~U(0.5,1.5), Tu~U(300,800) K, 20 steps "
+                       f"at dt 1e-8 s), 10% 2-D reactive shock tubes 512x128 (10 steps at dt 2e-8 s); 9 species",
+           "parallelism": f"replicas x{world}", "admission": "HBM budget 16 GiB, 32 grid slots, reactors "
+                                                           "batched per launch",
+           "l2": "mixed; latency-bound small solves"}
+    line = {"metric": S_METRIC, "value": stats["solves_per_s"] * world, "unit": S_METRIC, "n_gpus": world,
+            "steps": args.requests, "warmup": len(warm), "ms_per_step": 1e3 / stats["solves_per_s"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": cfg, "p50_s": stats["p50_s"], "p99_s": stats["p99_s"],
+            "by_kind": {k: stats[k] for k in ("reactor", "flame1d", "tube2d") if k in stats},
+            "max_grid_in_flight": stats["max_grid_in_flight"], "clocks": ck,
+            "e2e": {"value": stats["solves_per_s"] * world, "unit": S_METRIC, "path": "host Request objects in, "
+                    "host results out (every request's inputs are copied to and its results from the device)"}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference serves one solve per process; "
+                              "there is no served-mix counterpart to time"}), flush=True)
+            return 0
+        return run_serve(args)
+    if args.workload == "flame":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) != 0:
+                return 0
+            rate, cores, sample = cpu_flame(args)
+            print(json.dumps({"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC,
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "scaling": "weak",
+                              "vs_baseline": rate / FLAME_PUBLISHED, "dtype": "f64", "data": "synthetic (seeded)",
+                              "config": flame_config(args.gpus, 1),
+                              "cpu_baseline": {"value": rate, "unit": METRIC, "cores": cores, "kind": "port",
+                                               "sample": sample},
+                              "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
+        return run_flame(args)
     if args.workload == "reactors":
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) != 0:

@@ -181,6 +181,30 @@ int stx_compute_chemistry(stx_ctx *ctx, void *stream, double *w, double *w_aux, 
 int stx_rk_sync(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, int simpler);
 int stx_advance_solution(stx_ctx *ctx, void *stream, const stx_fields *f, double dt, double time);
 
+/* Precision form of a context.  STX_PREC_FP64 (the default) is the reference's
+ * FP64 method throughout.  STX_PREC_MIXED computes the central face fluxes,
+ * the viscous / heat / diffusion face fluxes and the transport properties
+ * (Wilke, Mathur, Bird) in FP32 and accumulates the RK residual in FP64; the
+ * T(e) Newton inversion, the WENO faces, the Arrhenius rates, K_c and the
+ * chemistry integration stay FP64.  The reference has no mixed form (it builds
+ * all-FP32 or all-FP64, SINGLE_PRECISION). */
+#define STX_PREC_FP64  0
+#define STX_PREC_MIXED 1
+int stx_set_precision(stx_ctx *ctx, int mode);
+
+/* Captured steps for fixed-dt runs (cfl < 0 in multideal.ini).  The reference
+ * launches ~50 kernels per step from its host loop (multideal_gpu.F90:1745-1806);
+ * stx_graph_create captures nsteps iterations of that loop (compute_aux(1,0),
+ * advance_solution, compute_aux(1,0), time += dt) into one CUDA graph on the
+ * fields f; stx_graph_launch sets the simulation time on the device and replays
+ * them on the stream (the chemistry windows read that time, so results equal the
+ * step-by-step calls bit for bit).  Requires iter_dt_recompute = 1.  The graph
+ * holds the field pointers and the context: keep both alive while it exists. */
+typedef struct stx_graph stx_graph;
+int stx_graph_create(stx_ctx *ctx, const stx_fields *f, double dt, int nsteps, stx_graph **out);
+int stx_graph_launch(stx_graph *g, void *stream, double time);
+int stx_graph_destroy(stx_graph *g);
+
 /* n independent adiabatic constant-pressure 0-D reactors integrated by ROK4 in
  * one persistent launch (work stealing over reactors).  The reference's batch
  * reactor (examples/batch_reactor, flow_init 8) is one constant-volume cell run

@@ -18,6 +18,8 @@ struct stx_ctx {
   unsigned int *status_d;         // device status word
   unsigned int *counter_d;        // work-stealing cell counter of the Rosenbrock kernels
   unsigned long long *dt_d;       // the nine CFL maxima
+  double *time_d;                 // simulation time of captured steps (stx_graph_*)
+  const DevCtx *dctx_d;           // device copy of d, for device functions that take the context by reference
   std::vector<void *> allocs;
   int device;
   // instrumentation (stx_profile_*)
@@ -273,9 +275,12 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   if ((rc = upload<unsigned int>(c, nullptr, 1, &st))) return fail(rc);
   if ((rc = upload<unsigned int>(c, nullptr, 1, &cn))) return fail(rc);
   if ((rc = upload<unsigned long long>(c, nullptr, 9, &dtp))) return fail(rc);
+  const double *tm = nullptr;
+  if ((rc = upload<double>(c, nullptr, 1, &tm))) return fail(rc);
   c->status_d = (unsigned int *)st;
   c->counter_d = (unsigned int *)cn;
   c->dt_d = (unsigned long long *)dtp;
+  c->time_d = (double *)tm;
   p.status = c->status_d;
   c->winf_d = nullptr;
   if (par->winf) {
@@ -284,6 +289,7 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
     c->winf_d = (double *)wf;
   }
   c->par.winf = nullptr;
+  if ((rc = upload<DevCtx>(c, &c->d, 1, &c->dctx_d))) return fail(rc);
   *out = c;
   return STX_OK;
 }
@@ -356,17 +362,17 @@ int stx_euler_x(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b,
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nx) return STX_E_INVALID;
   // reads Y, rho, u, v, w, h, p, c, Ducros (ns+8) and fl (unless overwritten); writes fl
   Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.ny * c->d.g.nz * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
-  return launch_euler(c->d, S(s), 0, wa, fl, a, b, ow);
+  return launch_euler(c->d, c->dctx_d, S(s), 0, wa, fl, a, b, ow);
 }
 int stx_euler_y(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.ny) return STX_E_INVALID;
   Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.nx * c->d.g.nz * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
-  return launch_euler(c->d, S(s), 1, wa, fl, a, b, ow);
+  return launch_euler(c->d, c->dctx_d, S(s), 1, wa, fl, a, b, ow);
 }
 int stx_euler_z(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nz) return STX_E_INVALID;
   Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.nx * c->d.g.ny * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
-  return launch_euler(c->d, S(s), 2, wa, fl, a, b, ow);
+  return launch_euler(c->d, c->dctx_d, S(s), 2, wa, fl, a, b, ow);
 }
 
 int stx_visflx(stx_ctx *c, void *s, const double *wa, double *fl, int mode) {
@@ -536,6 +542,92 @@ int stx_advance_solution(stx_ctx *c, void *s, const stx_fields *f, double dt, do
   } else {
     TRY(stx_rk_sync(c, s, f, dt, 0));
   }
+  return STX_OK;
+}
+
+int stx_set_precision(stx_ctx *c, int mode) {
+  if (!c || (mode != STX_PREC_FP64 && mode != STX_PREC_MIXED)) return STX_E_INVALID;
+  c->d.p.mixed = mode;
+  STX_CUDA_TRY(cudaMemcpy((void *)c->dctx_d, &c->d, sizeof(DevCtx), cudaMemcpyHostToDevice));
+  return STX_OK;
+}
+
+// ------------------------------------------------------------------ captured steps
+// A run at fixed dt (cfl < 0 in multideal.ini) repeats the same kernel sequence
+// every step; only the simulation time changes, and only the chemistry reads
+// it.  nsteps steps of the reference's integration loop
+// (multideal_gpu.F90:1745-1806: compute_aux, advance_solution, compute_aux;
+// the time advance) are captured once into a CUDA graph whose chemistry
+// kernels read the time from c->time_d and whose last node advances it, so
+// one graph launch replaces ~50 launches per step with the same arithmetic.
+struct stx_graph {
+  stx_ctx *c;
+  cudaGraphExec_t exec;
+  double dt;
+  int nsteps;
+};
+
+namespace {
+__global__ void k_time_add(double *t, double dt) { *t = *t + dt; }
+__global__ void k_time_set(double *t, double v) { *t = v; }
+}  // namespace
+
+int stx_graph_create(stx_ctx *c, const stx_fields *f, double dt, int nsteps, stx_graph **out) {
+  if (!c || !f || !out || nsteps < 1 || !(dt > 0.0)) return STX_E_INVALID;
+  *out = nullptr;
+  cudaStream_t cs;
+  STX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  const int prof = c->prof_on;
+  c->prof_on = 0;
+  c->d.p.time_d = c->time_d;
+  int rc = STX_OK;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) rc = STX_E_CUDA;
+  for (int n = 0; n < nsteps && rc == STX_OK; n++) {
+    if ((rc = stx_compute_aux(c, cs, f->w, f->w_aux, 1, 0))) break;
+    if ((rc = stx_advance_solution(c, cs, f, dt, 0.0))) break;
+    if ((rc = stx_compute_aux(c, cs, f->w, f->w_aux, 1, 0))) break;
+    k_time_add<<<1, 1, 0, cs>>>(c->time_d, dt);
+    if (cudaGetLastError() != cudaSuccess) rc = STX_E_CUDA;
+  }
+  if (e == cudaSuccess) {
+    cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+    if (e2 != cudaSuccess && rc == STX_OK) rc = STX_E_CUDA;
+  }
+  c->d.p.time_d = nullptr;
+  c->prof_on = prof;
+  stx_graph *g = nullptr;
+  if (rc == STX_OK) {
+    g = new (std::nothrow) stx_graph();
+    if (!g) rc = STX_E_NOMEM;
+  }
+  if (rc == STX_OK && cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) rc = STX_E_CUDA;
+  if (graph) cudaGraphDestroy(graph);
+  cudaStreamDestroy(cs);
+  if (rc != STX_OK) {
+    delete g;
+    return rc;
+  }
+  g->c = c;
+  g->dt = dt;
+  g->nsteps = nsteps;
+  *out = g;
+  return STX_OK;
+}
+
+int stx_graph_launch(stx_graph *g, void *s, double time) {
+  if (!g) return STX_E_INVALID;
+  k_time_set<<<1, 1, 0, S(s)>>>(g->c->time_d, time);
+  STX_CUDA_TRY(cudaGetLastError());
+  STX_CUDA_TRY(cudaGraphLaunch(g->exec, S(s)));
+  return STX_OK;
+}
+
+int stx_graph_destroy(stx_graph *g) {
+  if (!g) return STX_OK;
+  cudaGraphExecDestroy(g->exec);
+  delete g;
   return STX_OK;
 }
 

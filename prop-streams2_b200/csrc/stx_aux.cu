@@ -12,7 +12,7 @@
 // sqrt(mu_m)*(1/sqrt(mu_l)) and the constant pair factors 1/sqrt(1+W_l/W_m),
 // (W_m/W_l)^0.25 come from a host table; both change results only at rounding
 // level.  The species clip is stored only where it changes w.
-template <int NS>
+template <int NS, typename R>
 __global__ void __launch_bounds__(128) k_eval_aux(DevCtx c, double *__restrict__ w, double *__restrict__ wa,
                                                   int i0, int j0, int k0, int ni, int nj, int nk) {
   const DevGrid &g = c.g;
@@ -80,58 +80,58 @@ __global__ void __launch_bounds__(128) k_eval_aux(DevCtx c, double *__restrict__
   table_pos(t, tt, itt, dtt);
   const double *v0 = t.visc_r + (long long)(itt - 1) * NS, *v1 = v0 + NS;
   const double *l0 = t.lam_r + (long long)(itt - 1) * NS, *l1 = l0 + NS;
-  double mwmixt = t.Ru / rm;
-  double X[NS];
+  R mwmixt = (R)(t.Ru / rm);
+  R X[NS];
 #pragma unroll
-  for (int k2 = 0; k2 < NS; k2++) X[k2] = Y[k2] * mwmixt * ldg(t.mwinv + k2);
+  for (int k2 = 0; k2 < NS; k2++) X[k2] = (R)Y[k2] * mwmixt * (R)ldg(t.mwinv + k2);
   // Mathur
-  double k_cond = 0.0, k_cond2 = 0.0;
+  R k_cond = R(0.0), k_cond2 = R(0.0);
 #pragma unroll
   for (int k2 = 0; k2 < NS; k2++) {
-    double a = ldg(l0 + k2);
-    double klsp = a + (ldg(l1 + k2) - a) * dtt;
+    R a = (R)ldg(l0 + k2);
+    R klsp = a + ((R)ldg(l1 + k2) - a) * (R)dtt;
     k_cond = k_cond + X[k2] * klsp;
     k_cond2 = k_cond2 + X[k2] / klsp;
   }
-  k_cond = 0.5 * (k_cond + 1.0 / k_cond2);
+  k_cond = R(0.5) * (k_cond + R(1.0) / k_cond2);
   // Wilke
-  double muk[NS], smu[NS];
+  R muk[NS], smu[NS];
 #pragma unroll
   for (int k2 = 0; k2 < NS; k2++) {
-    double a = ldg(v0 + k2);
-    muk[k2] = a + (ldg(v1 + k2) - a) * dtt;
+    R a = (R)ldg(v0 + k2);
+    muk[k2] = a + ((R)ldg(v1 + k2) - a) * (R)dtt;
     smu[k2] = sqrt(muk[k2]);
   }
-  double mu = 0.0;
+  R mu = R(0.0);
 #pragma unroll
   for (int l = 0; l < NS; l++) {
-    double isl = 1.0 / smu[l];
-    double mu_den = 0.0;
+    R isl = R(1.0) / smu[l];
+    R mu_den = R(0.0);
 #pragma unroll
     for (int m = 0; m < NS; m++) {
-      double t1 = 1.0 + (smu[m] * isl) * ldg(t.wk_b + l * NS + m);
-      double phi_lm = ldg(t.wk_a + l * NS + m) * (t1 * t1);
-      mu_den = mu_den + Y[m] * phi_lm * ldg(t.mwinv + m);
+      R t1 = R(1.0) + (smu[m] * isl) * (R)ldg(t.wk_b + l * NS + m);
+      R phi_lm = (R)ldg(t.wk_a + l * NS + m) * (t1 * t1);
+      mu_den = mu_den + (R)Y[m] * phi_lm * (R)ldg(t.mwinv + m);
     }
-    mu = mu + muk[l] * Y[l] * ldg(t.mwinv + l) / mu_den;
+    mu = mu + muk[l] * (R)Y[l] * (R)ldg(t.mwinv + l) / mu_den;
   }
-  mu = sqrt(8.0) * mu;
-  FG(wa, p, J_MU) = mu;
-  FG(wa, p, J_K) = k_cond;
+  mu = (R)sqrt(8.0) * mu;
+  FG(wa, p, J_MU) = (double)mu;
+  FG(wa, p, J_K) = (double)k_cond;
   // Bird
   const double *d0 = t.diff_r + (long long)(itt - 1) * NS * NS, *d1 = d0 + NS * NS;
 #pragma unroll
   for (int l = 0; l < NS; l++) {
-    double diff_den = 0.0;
+    R diff_den = R(0.0);
 #pragma unroll
     for (int m = 0; m < NS; m++) {
       if (m != l) {
-        double a = ldg(d0 + l * NS + m);
-        double dij = a + (ldg(d1 + l * NS + m) - a) * dtt;
+        R a = (R)ldg(d0 + l * NS + m);
+        R dij = a + ((R)ldg(d1 + l * NS + m) - a) * (R)dtt;
         diff_den = diff_den + X[m] / dij;
       }
     }
-    FG(wa, p, J_K + 1 + l) = diff_den > 1.0e-15 ? (1.0 - Y[l]) / diff_den * c.p.p0 / pp * rho : 0.0;
+    FG(wa, p, J_K + 1 + l) = diff_den > R(1.0e-15) ? (double)((R)(1.0 - Y[l]) / diff_den) * c.p.p0 / pp * rho : 0.0;
   }
 }
 
@@ -370,7 +370,9 @@ static int eval_aux_t(const DevCtx &c, cudaStream_t s, double *w, double *wa, in
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   if (ni <= 0 || nj <= 0 || nk <= 0) return STX_OK;
   long long n = (long long)ni * nj * nk;
-  k_eval_aux<NS><<<grid1d(n, 128), 128, 0, s>>>(c, w, wa, i0, j0, k0, ni, nj, nk);
+  // transport properties: FP64 (plain form) or FP32 (mixed form)
+  if (c.p.mixed) k_eval_aux<NS, float><<<grid1d(n, 128), 128, 0, s>>>(c, w, wa, i0, j0, k0, ni, nj, nk);
+  else k_eval_aux<NS, double><<<grid1d(n, 128), 128, 0, s>>>(c, w, wa, i0, j0, k0, ni, nj, nk);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }

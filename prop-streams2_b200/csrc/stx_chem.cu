@@ -19,13 +19,17 @@
 #endif
 
 template <int NS>
-__global__ void __launch_bounds__(STX_CHEM_BLOCK, STX_ROK4_MINB)
+__global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
     k_rok4(DevCtx c, double *__restrict__ w, const double *__restrict__ wa,
                                               const double *__restrict__ fl_sav, double dttry, double t0, double t1,
                                               int simpler, unsigned int *counter) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
   const double eps_Z = 5e-4;
+  if (c.p.time_d) {                 // captured step: the window starts at the device-held time
+    t0 = *c.p.time_d;
+    t1 = t0 + dttry;
+  }
   for (;;) {
     long long cell = claim(counter);
     if (cell >= g.npi) break;
@@ -53,7 +57,7 @@ __global__ void __launch_bounds__(STX_CHEM_BLOCK, STX_ROK4_MINB)
 // times, so their step counts differ by orders of magnitude).  Y0 / Y are
 // (n, ns) with the reactor index fastest.
 template <int NS>
-__global__ void __launch_bounds__(STX_CHEM_BLOCK, STX_ROK4_MINB)
+__global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
     k_batch0d(DevCtx c, int n, const double *__restrict__ T0, const double *__restrict__ p0,
               const double *__restrict__ Y0, double t_max, double dttry, double ign_factor, double end_factor,
               double *__restrict__ Y, double *__restrict__ T, double *__restrict__ t_ign, double *__restrict__ t_end,
@@ -246,6 +250,10 @@ __global__ void __launch_bounds__(128) k_rosenbrock(DevCtx c, double *__restrict
                                                     double dttry, double t0, double t1, unsigned int *counter) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
+  if (c.p.time_d) {                 // captured step: the window starts at the device-held time
+    t0 = *c.p.time_d;
+    t1 = t0 + dttry;
+  }
   for (;;) {
     long long cell = claim(counter);
     if (cell >= g.npi) break;
@@ -322,10 +330,10 @@ template <int NS>
 static int rok4_t(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
                   double t0, double t1, int simpler, unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
-  int nb = persistent_blocks((const void *)k_rok4<NS>, STX_CHEM_BLOCK);
-  long long need = (c.g.npi + STX_CHEM_BLOCK - 1) / STX_CHEM_BLOCK;
+  int nb = persistent_blocks((const void *)k_rok4<NS>, chem_block(NS));
+  long long need = (c.g.npi + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
-  k_rok4<NS><<<nb, STX_CHEM_BLOCK, 0, s>>>(c, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
+  k_rok4<NS><<<nb, chem_block(NS), 0, s>>>(c, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
@@ -357,10 +365,10 @@ static int batch0d_t(const DevCtx &c, cudaStream_t s, int n, const double *T0, c
                      double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
                      double *t_end, int *nsteps, unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
-  int nb = persistent_blocks((const void *)k_batch0d<NS>, STX_CHEM_BLOCK);
-  long long need = ((long long)n + STX_CHEM_BLOCK - 1) / STX_CHEM_BLOCK;
+  int nb = persistent_blocks((const void *)k_batch0d<NS>, chem_block(NS));
+  long long need = ((long long)n + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
-  k_batch0d<NS><<<nb, STX_CHEM_BLOCK, 0, s>>>(c, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps,
+  k_batch0d<NS><<<nb, chem_block(NS), 0, s>>>(c, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps,
                                               counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;

@@ -4,8 +4,6 @@
 #pragma once
 #include "stx_kernels.cuh"
 
-// Threads per CTA of the chemistry kernels (per-thread shared-memory rows).
-#define STX_CHEM_BLOCK 128
 
 // Temperature-table position of T for K_c (kernels_gpu.F90:9259-9264).
 __device__ __forceinline__ void kc_pos(const DevTab &t, double tt, int &itt, double &dtt) {
@@ -184,7 +182,7 @@ __device__ void chem_source_sp(const DevTab &t, double tt, const double *conc, d
 // the ROK4 loop stays small enough for the instruction cache.  With the
 // context's tables (KCF false) the production terms run over the sparse
 // stoichiometry with per-thread rows in shared memory (launch with
-// STX_CHEM_BLOCK threads); with the reference's raw tables (KCF true) over the
+// chem_block(NS) threads); with the reference's raw tables (KCF true) over the
 // dense species loops.
 template <int NS, bool KCF = false>
 __device__ __noinline__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, double *rhs) {
@@ -210,16 +208,17 @@ __device__ __noinline__ void krylov_rhs(const DevCtx &c, const double *w_sav, do
   if (KCF) {
     chem_source<NS, KCF>(t, tt, conc, rhs, false);
   } else {
-    __shared__ double s_conc[NS * STX_CHEM_BLOCK], s_rhs[NS * STX_CHEM_BLOCK];
+    constexpr int CB = chem_block(NS);
+    __shared__ double s_conc[NS * CB], s_rhs[NS * CB];
     double *cs = s_conc + threadIdx.x, *rs = s_rhs + threadIdx.x;
 #pragma unroll
     for (int k = 0; k < NS; k++) {
-      cs[k * STX_CHEM_BLOCK] = conc[k];
-      rs[k * STX_CHEM_BLOCK] = 0.0;
+      cs[k * CB] = conc[k];
+      rs[k * CB] = 0.0;
     }
-    chem_source_sp<NS, STX_CHEM_BLOCK>(t, tt, cs, rs);
+    chem_source_sp<NS, CB>(t, tt, cs, rs);
 #pragma unroll
-    for (int k = 0; k < NS; k++) rhs[k] = rs[k * STX_CHEM_BLOCK];
+    for (int k = 0; k < NS; k++) rhs[k] = rs[k * CB];
   }
 }
 
@@ -320,7 +319,6 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
   const double bsv[4] = {bs1, bs2, bs3, bs4}, btv[4] = {bt1, bt2, bt3, bt4};
   double V[NV * (STX_MMAX + 1)];
   double inv[STX_MMAX * STX_MMAX];
-  double Am[NV * STX_MMAX];
   double Ks[NV * STX_NSTAGE];
   double rhs_sav[NV];
   int mA = 0;
@@ -398,21 +396,11 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
         }
       }
     }
-    // ---- A = Vb (I - inv)  (Vb = first mA columns of V, zero beyond)
-#pragma unroll 1
-    for (int kk = 1; kk <= STX_MMAX; kk++)
-#pragma unroll 1
-      for (int ll = 0; ll < NV; ll++) {
-        double idf = ((1 == kk) ? 1.0 : 0.0) - inv[(kk - 1) * STX_MMAX + 0];
-        double a = (mA >= 1 ? V[ll] : 0.0) * idf;
-        for (int jj = 2; jj <= STX_MMAX; jj++) {
-          double vb = (jj <= mA) ? V[(jj - 1) * NV + ll] : 0.0;
-          idf = ((jj == kk) ? 1.0 : 0.0) - inv[(kk - 1) * STX_MMAX + jj - 1];
-          a = a + vb * idf;
-        }
-        Am[(kk - 1) * NV + ll] = a;
-      }
-    // ---- stages; B(ll,jj) = sum_q A(ll,q) Vb(jj,q) is recomputed where used
+    // ---- stages.  The reference forms A = Vb (I - inv) and B = A Vb^T (nv x nv)
+    // and applies B to F (:10540-10566).  Here B F = A (Vb^T F): the mA
+    // projections of F on the basis first, then per row the 4 entries of A,
+    // formed in registers from V and inv.  O(4 nv) instead of O(4 nv^2) per
+    // stage; the sums are regrouped (rounding-level difference).
 #pragma unroll 1
     for (int ii = 1; ii <= STX_NSTAGE; ii++) {
       double ys[NV], F[NV], GK[NV];
@@ -428,13 +416,26 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
       for (int m = 0; m < NV; m++) F[m] = F[m] + GK[m];
       if (simpler == 1)
         for (int m = 0; m < NV; m++) F[m] = F[m] - fls[m];
+      double pf[STX_MMAX];
+#pragma unroll
+      for (int q = 0; q < STX_MMAX; q++) {
+        double s = 0.0;
+        if (q < mA)
+          for (int jj = 0; jj < NV; jj++) s = s + V[q * NV + jj] * F[jj];
+        pf[q] = s;
+      }
 #pragma unroll 1
       for (int ll = 0; ll < NV; ll++) {
+        double vb[STX_MMAX];
+#pragma unroll
+        for (int q = 0; q < STX_MMAX; q++) vb[q] = (q < mA) ? V[q * NV + ll] : 0.0;
         double s = 0.0;
-        for (int jj = 0; jj < NV; jj++) {
-          double b = Am[ll] * (mA >= 1 ? V[jj] : 0.0);
-          for (int q = 2; q <= STX_MMAX; q++) b = b + Am[(q - 1) * NV + ll] * ((q <= mA) ? V[(q - 1) * NV + jj] : 0.0);
-          s = (jj == 0) ? b * F[0] : s + b * F[jj];
+#pragma unroll
+        for (int kk = 0; kk < STX_MMAX; kk++) {
+          double a = vb[0] * ((kk == 0 ? 1.0 : 0.0) - inv[kk * STX_MMAX + 0]);
+#pragma unroll
+          for (int jj = 1; jj < STX_MMAX; jj++) a = a + vb[jj] * ((jj == kk ? 1.0 : 0.0) - inv[kk * STX_MMAX + jj]);
+          s = s + a * pf[kk];
         }
         Ks[(ii - 1) * NV + ll] = F[ll] - s - GK[ll];
       }
@@ -492,7 +493,7 @@ struct Rok4Flow {
 // evaluated; h and p fixed; T from h by the Newton iteration of
 // get_mixture_temperature_from_h_roe_dev (kernels_gpu.F90:6810-6900);
 // rho = p / (R T); dY_k/dt = W_k omega_k / rho.  Per-thread shared-memory rows
-// as in krylov_rhs (launch with STX_CHEM_BLOCK threads).
+// as in krylov_rhs (launch with chem_block(NS) threads).
 template <int NS>
 __device__ __noinline__ void cp_rhs(const DevCtx &c, const double *y, double T_iter, double h, double p,
                                     double *out) {
@@ -505,16 +506,17 @@ __device__ __noinline__ void cp_rhs(const DevCtx &c, const double *y, double T_i
 #pragma unroll
   for (int k = 0; k < NS; k++) rm = rm + ldg(t.rgas + k) * Yc[k];
   double rho = p / (rm * tt);
-  __shared__ double s_conc[NS * STX_CHEM_BLOCK], s_rhs[NS * STX_CHEM_BLOCK];
+  constexpr int CB = chem_block(NS);
+  __shared__ double s_conc[NS * CB], s_rhs[NS * CB];
   double *cs = s_conc + threadIdx.x, *rs = s_rhs + threadIdx.x;
 #pragma unroll
   for (int k = 0; k < NS; k++) {
-    cs[k * STX_CHEM_BLOCK] = rho * Yc[k] / ldg(t.mw + k);
-    rs[k * STX_CHEM_BLOCK] = 0.0;
+    cs[k * CB] = rho * Yc[k] / ldg(t.mw + k);
+    rs[k * CB] = 0.0;
   }
-  chem_source_sp<NS, STX_CHEM_BLOCK>(t, tt, cs, rs);
+  chem_source_sp<NS, CB>(t, tt, cs, rs);
 #pragma unroll
-  for (int k = 0; k < NS; k++) out[k] = rs[k * STX_CHEM_BLOCK] / rho;
+  for (int k = 0; k < NS; k++) out[k] = rs[k * CB] / rho;
 }
 
 template <int NS>

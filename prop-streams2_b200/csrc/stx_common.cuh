@@ -16,7 +16,13 @@
 #define STX_SPW (4 * STX_SPR)   // sparse row: reactants, products, union (2 STX_SPR)
 
 // species counts compiled into the library
-#define STX_FOR_NS(X) X(9) X(11) X(13) X(14)
+#define STX_FOR_NS(X) X(9) X(11) X(13) X(14) X(53)
+
+// CTA sizes of the kernels that keep NS-long per-thread rows (chemistry) or
+// (NS+4)-long per-face rows (the x sweeps) in shared memory: smaller CTAs for
+// large mechanisms keep the static shared memory under 48 KB.
+__host__ __device__ constexpr int chem_block(int ns) { return ns > 20 ? 32 : 128; }
+__host__ __device__ constexpr int xsweep_block(int ns) { return ns > 20 ? 64 : 128; }
 
 struct DevTab {
   int ns, nr, icl, icr, nset, ntab, ncp;
@@ -57,6 +63,15 @@ struct DevPar {
   int ros_maxsteps, ros_maxtry;
   double cd1[5][5];               // coeff_deriv1(l, lmax) -> cd1[l][lmax]
   unsigned int *status;           // device status word
+  // Simulation time in device memory, set only while a step is captured into a
+  // CUDA graph: the chemistry kernels then take their window [time, time + dttry]
+  // from it (the same double operations the host performs) instead of their
+  // t0 / t1 arguments, so a replayed step sees the current time.
+  const double *time_d;
+  // precision form: 0 plain FP64; 1 mixed -- central face fluxes, viscous and
+  // diffusive fluxes and the transport properties in FP32 (RK residual still
+  // accumulated in FP64; T(e) Newton, rates, K_c and the chemistry in FP64)
+  int mixed;
 };
 
 struct DevCtx {

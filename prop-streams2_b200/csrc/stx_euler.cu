@@ -3,12 +3,16 @@
 // kernels of src/multideal/kernels_gpu.F90:88-2063, 2065-3295).
 //
 // B200 design:
-//  * x sweep: one CTA of 128 threads per pencil segment; thread t computes face
-//    f0+t, the faces go through shared memory and threads 1..127 apply
-//    fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- no fhat round trip through HBM.
+//  * x sweep: the faces of all rows numbered as one sequence, 128 per CTA (one
+//    shared with the next CTA); the faces go through shared memory and the
+//    threads apply fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- no fhat round
+//    trip through HBM.
 //  * y/z sweeps: tiles of 32 contiguous i (coalesced) x 8 faces along the
 //    sweep, one face per thread, differenced through shared memory; one
 //    redundant face per 7 cells.
+//  * In every sweep the central faces are computed in place and the faces the
+//    Ducros test sends to WENO are gathered per CTA and worked through by full
+//    warps.
 //  * WENO faces use the structure of the multi-species eigenvectors
 //    (kernels_gpu.F90:2703-2984): the species block of L is identity + rank one,
 //    so every characteristic variable follows from two per-point scalars
@@ -146,11 +150,14 @@ __device__ __forceinline__ double weno_rec(const double *vp, const double *vm, i
 #define CF_LMAX 4                            // largest ep_order / 2 (coeff_deriv1 is 4 x 4)
 #define CF_NPAIR (CF_LMAX * (CF_LMAX + 1) / 2)   // stencil pairs (l, m), m < l <= CF_LMAX
 
-// Central KEEP(n) face flux (kernels_gpu.F90:145-337 and the y/z copies).
-template <int NS, int DIR>
+// Central KEEP(n) face flux (kernels_gpu.F90:145-337 and the y/z copies), computed
+// in R: double for the plain form, float for the mixed form (the fields are
+// read in FP64 and rounded once).
+template <int NS, int DIR, typename R>
 __device__ __forceinline__ void central_flux(const DevCtx &c, const double *__restrict__ wa, long long p, long long st,
-                                             bool fz, double *fh) {
+                                             bool fz, R *fh) {
   const DevGrid &g = c.g;
+  auto ld = [&](long long q, int m) -> R { return (R)FG(wa, q, m); };
   const int J_U = NS + 1, J_V = NS + 2, J_W = NS + 3, J_H = NS + 4, J_P = NS + 6, J_R = NS + 11;
   const int Jn = J_U + DIR;
   int lmax = c.p.ep_order / 2;
@@ -162,80 +169,80 @@ __device__ __forceinline__ void central_flux(const DevCtx &c, const double *__re
   // momentum/energy fluxes share.  The reference forms it inside its species
   // loop (the KEEP density factor drhof depends on rho_a, rho_b only); it is
   // formed once per pair here, with the same operations.
-  double up[CF_NPAIR];
+  R up[CF_NPAIR];
 #pragma unroll
   for (int l = 1; l <= CF_LMAX; l++)
 #pragma unroll
     for (int m = 0; m < l; m++) {
       const int q = l * (l - 1) / 2 + m;
-      up[q] = 0.0;
+      up[q] = R(0.0);
       if (l <= lmax) {
         long long a = p - m * st, b = p + (l - m) * st;
-        double rhoi = FG(wa, a, J_R), uni = FG(wa, a, Jn);
-        double rhoip = FG(wa, b, J_R), unip = FG(wa, b, Jn);
-        double rhom = rhoi + rhoip, drhof;
+        R rhoi = ld(a, J_R), uni = ld(a, Jn);
+        R rhoip = ld(b, J_R), unip = ld(b, Jn);
+        R rhom = rhoi + rhoip, drhof;
         if (nkeep <= 0) {
-          drhof = 1.0;
+          drhof = R(1.0);
         } else {
-          double drho = 2.0 * (rhoip - rhoi) / rhom;
-          double t = (0.5 * drho) * (0.5 * drho), t2 = t;
-          double sumden = 1.0 + t / 3.0;
-          for (int n = 2; n <= nkeep; n++) { int n2 = 2 * n; t = t2 * t; sumden = sumden + t / (1.0 + n2); }
-          drhof = 1.0 / sumden;
+          R drho = R(2.0) * (rhoip - rhoi) / rhom;
+          R t = (R(0.5) * drho) * (R(0.5) * drho), t2 = t;
+          R sumden = R(1.0) + t / R(3.0);
+          for (int n = 2; n <= nkeep; n++) { int n2 = 2 * n; t = t2 * t; sumden = sumden + t / (R(1.0) + n2); }
+          drhof = R(1.0) / sumden;
         }
         up[q] = (uni + unip) * rhom * drhof;
       }
     }
 #pragma unroll 1
   for (int lsp = 1; lsp <= NS; lsp++) {
-    double ft1 = 0.0;
+    R ft1 = R(0.0);
 #pragma unroll
     for (int l = 1; l <= CF_LMAX; l++) {
       if (l <= lmax) {
-        double uvs1 = 0.0;
+        R uvs1 = R(0.0);
 #pragma unroll
         for (int m = 0; m < l; m++) {
           long long a = p - m * st, b = p + (l - m) * st;
-          uvs1 = uvs1 + up[l * (l - 1) / 2 + m] * (FG(wa, a, lsp) + FG(wa, b, lsp));
+          uvs1 = uvs1 + up[l * (l - 1) / 2 + m] * (ld(a, lsp) + ld(b, lsp));
         }
-        ft1 = ft1 + c.p.cd1[l][lmax] * uvs1;
+        ft1 = ft1 + R(c.p.cd1[l][lmax]) * uvs1;
       }
     }
-    double fh1 = 0.25 * ft1;
-    fh[lsp - 1] = fz ? 0.0 : fh1;
+    R fh1 = R(0.25) * ft1;
+    fh[lsp - 1] = fz ? R(0.0) : fh1;
   }
-  double ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
+  R ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
 #pragma unroll
   for (int l = 1; l <= CF_LMAX; l++) {
     if (l > lmax) break;
-    double uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs6 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0;
+    R uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs6 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0;
 #pragma unroll
     for (int m = 0; m < l; m++) {
       const int q = l * (l - 1) / 2 + m;
       long long a = p - m * st, b = p + (l - m) * st;
-      double rhoi = FG(wa, a, J_R), uui = FG(wa, a, J_U), vvi = FG(wa, a, J_V), wwi = FG(wa, a, J_W);
-      double enti = FG(wa, a, J_H), ppi = FG(wa, a, J_P);
-      double rhoip = FG(wa, b, J_R), uuip = FG(wa, b, J_U), vvip = FG(wa, b, J_V), wwip = FG(wa, b, J_W);
-      double entip = FG(wa, b, J_H), ppip = FG(wa, b, J_P);
-      double uni = DIR == 0 ? uui : (DIR == 1 ? vvi : wwi);
-      double unip = DIR == 0 ? uuip : (DIR == 1 ? vvip : wwip);
-      double uv_part = up[q];
+      R rhoi = ld(a, J_R), uui = ld(a, J_U), vvi = ld(a, J_V), wwi = ld(a, J_W);
+      R enti = ld(a, J_H), ppi = ld(a, J_P);
+      R rhoip = ld(b, J_R), uuip = ld(b, J_U), vvip = ld(b, J_V), wwip = ld(b, J_W);
+      R entip = ld(b, J_H), ppip = ld(b, J_P);
+      R uni = DIR == 0 ? uui : (DIR == 1 ? vvi : wwi);
+      R unip = DIR == 0 ? uuip : (DIR == 1 ? vvip : wwip);
+      R uv_part = up[q];
       if (nkeep >= 0) {
-        double eei = enti - ppi / rhoi - 0.5 * (uui * uui + vvi * vvi + wwi * wwi);
-        double eeip = entip - ppip / rhoip - 0.5 * (uuip * uuip + vvip * vvip + wwip * wwip);
-        double eem = eei + eeip, deef;
+        R eei = enti - ppi / rhoi - R(0.5) * (uui * uui + vvi * vvi + wwi * wwi);
+        R eeip = entip - ppip / rhoip - R(0.5) * (uuip * uuip + vvip * vvip + wwip * wwip);
+        R eem = eei + eeip, deef;
         if (nkeep == 0) {
-          deef = 1.0;
+          deef = R(1.0);
         } else {
-          double dee = 2.0 * (eeip - eei) / eem;
-          double te = (0.5 * dee) * (0.5 * dee);
-          double te2 = te;
-          double sde = 1.0 + te, sne = 1.0 + te / 3.0;
+          R dee = R(2.0) * (eeip - eei) / eem;
+          R te = (R(0.5) * dee) * (R(0.5) * dee);
+          R te2 = te;
+          R sde = R(1.0) + te, sne = R(1.0) + te / R(3.0);
           for (int n = 2; n <= nkeep; n++) {
             int n2 = 2 * n;
             te = te2 * te;
             sde = sde + te;
-            sne = sne + te / (1.0 + n2);
+            sne = sne + te / (R(1.0) + n2);
           }
           deef = sne / sde;
         }
@@ -244,28 +251,28 @@ __device__ __forceinline__ void central_flux(const DevCtx &c, const double *__re
         uvs4 = uvs4 + uv_part * (wwi + wwip);
         uvs5_i = uvs5_i + uv_part * eem * deef;
         uvs5_k = uvs5_k + uv_part * (uui * uuip + vvi * vvip + wwi * wwip);
-        uvs5_p = uvs5_p + 4.0 * (uni * ppip + unip * ppi);
-        uvs6 = uvs6 + (2.0) * (ppi + ppip);
+        uvs5_p = uvs5_p + R(4.0) * (uni * ppip + unip * ppi);
+        uvs6 = uvs6 + (R(2.0)) * (ppi + ppip);
       } else {
         uvs2 = uvs2 + uv_part * (uui + uuip);
         uvs3 = uvs3 + uv_part * (vvi + vvip);
         uvs4 = uvs4 + uv_part * (wwi + wwip);
         uvs5 = uvs5 + uv_part * (enti + entip);
-        uvs6 = uvs6 + (2.0) * (ppi + ppip);
+        uvs6 = uvs6 + (R(2.0)) * (ppi + ppip);
       }
     }
-    double cl = c.p.cd1[l][lmax];
+    R cl = R(c.p.cd1[l][lmax]);
     ft2 = ft2 + cl * uvs2;
     ft3 = ft3 + cl * uvs3;
     ft4 = ft4 + cl * uvs4;
     ft5 = ft5 + cl * (nkeep >= 0 ? (uvs5_i + uvs5_k + uvs5_p) : uvs5);
     ft6 = ft6 + cl * uvs6;
   }
-  double fm0 = 0.25 * ft2, fm1 = 0.25 * ft3, fm2 = 0.25 * ft4, fh5 = 0.25 * ft5;
-  if (fz) { fm0 = fm1 = fm2 = fh5 = 0.0; }
-  if (DIR == 0) fm0 = fm0 + 0.5 * ft6;
-  if (DIR == 1) fm1 = fm1 + 0.5 * ft6;
-  if (DIR == 2) fm2 = fm2 + 0.5 * ft6;
+  R fm0 = R(0.25) * ft2, fm1 = R(0.25) * ft3, fm2 = R(0.25) * ft4, fh5 = R(0.25) * ft5;
+  if (fz) { fm0 = fm1 = fm2 = fh5 = R(0.0); }
+  if (DIR == 0) fm0 = fm0 + R(0.5) * ft6;
+  if (DIR == 1) fm1 = fm1 + R(0.5) * ft6;
+  if (DIR == 2) fm2 = fm2 + R(0.5) * ft6;
   fh[NS] = fm0; fh[NS + 1] = fm1; fh[NS + 2] = fm2; fh[NS + 3] = fh5;
 }
 
@@ -520,48 +527,84 @@ __device__ __noinline__ void weno_rusanov_flux(const DevCtx &c, const double *__
   }
 }
 
-// Hybrid face flux: Ducros test over the WENO stencil, then central or upwind.
-template <int NS, int DIR>
-__device__ __forceinline__ void face_flux(const DevCtx &c, const double *__restrict__ wa, long long p, long long st,
-                                          int face, int nmax, double *fh) {
+// Hybrid face flux (kernels_gpu.F90:88-2063): the Ducros test over the WENO
+// stencil picks the central KEEP flux or the upwind (characteristic or
+// Rusanov) WENO flux.  The sweeps evaluate the test for every face first, do
+// the central faces in place, and gather the shocked faces of the CTA into a
+// list that full warps then work through, so that a few WENO faces do not
+// stall every warp they fall in.
+template <int NS>
+__device__ __forceinline__ bool face_shocked(const DevCtx &c, const double *__restrict__ wa, long long p, long long st) {
   const DevGrid &g = c.g;
   const int J_DUC = NS + 9;
   const int ws = c.p.weno_scheme;
   bool shk = false;
   for (int s = -ws + 1; s <= ws; s++) shk |= (FG(wa, p + s * st, J_DUC) > c.p.sensor_threshold);
-  if (!shk) {
-    bool fz = (face == 0 && c.p.fzf[2 * DIR] == 1) || (face == nmax && c.p.fzf[2 * DIR + 1] == 1);
-    central_flux<NS, DIR>(c, wa, p, st, fz, fh);
-  } else if (c.p.flux_splitting == 1) {
-    weno_rusanov_flux<NS, DIR>(c, wa, p, st, fh);
-  } else {
-    weno_char_flux<NS, DIR>(c, wa, p, st, fh);
-  }
+  return shk;
+}
+
+template <int NS, int DIR, typename R>
+__device__ __forceinline__ void weno_face(const DevCtx &c, const DevCtx *__restrict__ cg,
+                                          const double *__restrict__ wa, long long p, long long st, R *fh) {
+  // The out-of-line WENO fluxes take the context by reference and write
+  // through a pointer.  They get the device-resident copy cg of the context
+  // (the by-value kernel parameter c would otherwise be copied to local memory
+  // by every thread) and their own output array.
+  double fw[NS + 4];
+  if (c.p.flux_splitting == 1) weno_rusanov_flux<NS, DIR>(*cg, wa, p, st, fw);
+  else weno_char_flux<NS, DIR>(*cg, wa, p, st, fw);
+#pragma unroll
+  for (int m = 0; m < NS + 4; m++) fh[m] = (R)fw[m];
 }
 
 // x sweep: the faces nmin-1..nmax of every (j, k) row are numbered as one
-// sequence F = row * nf + (f - nmin + 1); CTA b computes faces 127 b .. 127 b + 127
+// sequence F = row * nf + (f - nmin + 1); CTA b of XB threads computes faces
+// (XB - 1) b .. (XB - 1) b + XB - 1
 // (one face shared with the next CTA), puts them in shared memory, and the
 // threads whose face is not the first of its row form
 // fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- every thread busy for any nx.
-template <int NS>
-__global__ void __launch_bounds__(128, 4) k_euler_x(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl,
+template <int NS, typename R>
+__global__ void __launch_bounds__(128, 4) k_euler_x(DevCtx c, const DevCtx *__restrict__ cg,
+                                                    const double *__restrict__ wa, double *__restrict__ fl,
                                                     int nmin, int nmax, int overwrite) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
-  __shared__ double sf[NV][128];
+  constexpr int XB = xsweep_block(NS);
+  __shared__ R sf[NV][XB];
+  __shared__ int wlist[XB];
+  __shared__ int nw;
+  if (threadIdx.x == 0) nw = 0;
+  __syncthreads();
   const long long nf = nmax - nmin + 2;
-  const long long F = (long long)blockIdx.x * 127 + threadIdx.x;
-  const bool act = F < nf * g.ny * g.nz;
+  const long long ntot = nf * g.ny * g.nz;
+  const long long F = (long long)blockIdx.x * (XB - 1) + threadIdx.x;
+  const bool act = F < ntot;
   const long long row = F / nf;
   const int f = nmin - 1 + (int)(F - row * nf);
   const int j = 1 + (int)(row % g.ny), k = 1 + (int)(row / g.ny);
   if (act) {
-    double fh[NV];
     long long p = gidx(g, f, j, k);
-    face_flux<NS, 0>(c, wa, p, 1, f, g.nx, fh);
+    if (!face_shocked<NS>(c, wa, p, 1)) {
+      R fh[NV];
+      bool fz = (f == 0 && c.p.fzf[0] == 1) || (f == g.nx && c.p.fzf[1] == 1);
+      central_flux<NS, 0, R>(c, wa, p, 1, fz, fh);
 #pragma unroll
-    for (int m = 0; m < NV; m++) sf[m][threadIdx.x] = fh[m];
+      for (int m = 0; m < NV; m++) sf[m][threadIdx.x] = fh[m];
+    } else {
+      wlist[atomicAdd(&nw, 1)] = threadIdx.x;
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nw; q += XB) {
+    const int t = wlist[q];
+    const long long Ft = (long long)blockIdx.x * (XB - 1) + t;
+    const long long rt = Ft / nf;
+    const int ft = nmin - 1 + (int)(Ft - rt * nf);
+    const long long p = gidx(g, ft, 1 + (int)(rt % g.ny), 1 + (int)(rt / g.ny));
+    R fh[NV];
+    weno_face<NS, 0, R>(c, cg, wa, p, 1, fh);
+#pragma unroll
+    for (int m = 0; m < NV; m++) sf[m][t] = fh[m];
   }
   __syncthreads();
   if (threadIdx.x >= 1 && act && f >= nmin) {
@@ -570,7 +613,7 @@ __global__ void __launch_bounds__(128, 4) k_euler_x(DevCtx c, const double *__re
     double met = ldg(g.dcsidx + i - 1);
 #pragma unroll
     for (int m = 0; m < NV; m++) {
-      double d = (sf[m][threadIdx.x] - sf[m][threadIdx.x - 1]) * met;
+      double d = (double)((sf[m][threadIdx.x] - sf[m][threadIdx.x - 1]) * (R)met);
       FI(fl, q, m + 1) = overwrite ? d : FI(fl, q, m + 1) + d;
     }
   }
@@ -580,15 +623,24 @@ __global__ void __launch_bounds__(128, 4) k_euler_x(DevCtx c, const double *__re
 // by YZ_TF consecutive faces of the sweep; every thread computes one face, the
 // faces go through shared memory, and rows 1..YZ_TF-1 form the YZ_TF-1 cells
 // fl(f) += (fhat_f - fhat_{f-1}) * d(eta)/dy.  One redundant face per tile.
-#define YZ_TI 32
-#define YZ_TF 8
-template <int NS, int DIR>
-__global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const double *__restrict__ wa,
-                                                           double *__restrict__ fl, int nmin, int nmax, int overwrite) {
+// (YZ_TI, YZ_TF) = (32, 8); (16, 6) for large mechanisms (shared memory)
+template <int NS> struct YZTile {
+  static constexpr int TI = NS > 20 ? 16 : 32, TF = NS > 20 ? 6 : 8;
+};
+#define YZ_TI (YZTile<NS>::TI)
+#define YZ_TF (YZTile<NS>::TF)
+template <int NS, int DIR, typename R>
+__global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const DevCtx *__restrict__ cg,
+                                                           const double *__restrict__ wa, double *__restrict__ fl,
+                                                           int nmin, int nmax, int overwrite) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
-  __shared__ double sf[NV][YZ_TF][YZ_TI];
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  __shared__ R sf[NV][YZ_TF][YZ_TI];
+  __shared__ int wlist[YZ_TF * YZ_TI];
+  __shared__ int nw;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * YZ_TI + tx;
+  if (tid == 0) nw = 0;
+  __syncthreads();
   int i = blockIdx.x * YZ_TI + tx + 1;
   int tr = blockIdx.y + 1;                 // k for the y sweep, j for the z sweep
   int f = nmin - 1 + blockIdx.z * (YZ_TF - 1) + ty;
@@ -596,11 +648,26 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const doub
   int nsw = DIR == 1 ? g.ny : g.nz;
   bool act = i <= g.nx && f <= nmax;
   if (act) {
-    double fh[NV];
     long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
-    face_flux<NS, DIR>(c, wa, p, st, f, nsw, fh);
+    if (!face_shocked<NS>(c, wa, p, st)) {
+      R fh[NV];
+      bool fz = (f == 0 && c.p.fzf[2 * DIR] == 1) || (f == nsw && c.p.fzf[2 * DIR + 1] == 1);
+      central_flux<NS, DIR, R>(c, wa, p, st, fz, fh);
 #pragma unroll
-    for (int m = 0; m < NV; m++) sf[m][ty][tx] = fh[m];
+      for (int m = 0; m < NV; m++) sf[m][ty][tx] = fh[m];
+    } else {
+      wlist[atomicAdd(&nw, 1)] = tid;
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < nw; q += YZ_TF * YZ_TI) {
+    const int t = wlist[q], sx = t % YZ_TI, sy = t / YZ_TI;
+    const int it = blockIdx.x * YZ_TI + sx + 1, ft = nmin - 1 + blockIdx.z * (YZ_TF - 1) + sy;
+    const long long p = DIR == 1 ? gidx(g, it, ft, tr) : gidx(g, it, tr, ft);
+    R fh[NV];
+    weno_face<NS, DIR, R>(c, cg, wa, p, st, fh);
+#pragma unroll
+    for (int m = 0; m < NV; m++) sf[m][sy][sx] = fh[m];
   }
   __syncthreads();
   if (ty >= 1 && act) {
@@ -609,36 +676,47 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const doub
     double mt = ldg(met + f - 1);
 #pragma unroll
     for (int m = 0; m < NV; m++) {
-      double d = (sf[m][ty][tx] - sf[m][ty - 1][tx]) * mt;
+      double d = (double)((sf[m][ty][tx] - sf[m][ty - 1][tx]) * (R)mt);
       FI(fl, q, m + 1) = overwrite ? d : FI(fl, q, m + 1) + d;
     }
   }
 }
 
-template <int NS>
-static int euler_t(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl, int nmin, int nmax, int ow) {
+template <int NS, typename R>
+static int euler_r(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
+                   int nmax, int ow) {
   const DevGrid &g = c.g;
   if (nmax - nmin < 0) return STX_OK;
   if (2 * c.p.weno_scheme > WMAX) return STX_E_UNSUPPORTED;
   if (dir == 0) {
     long long nface = (long long)(nmax - nmin + 2) * g.ny * g.nz;
-    long long nb = (nface - 1 + 126) / 127;     // CTA b covers faces 127 b .. 127 b + 127
+    constexpr int XB = xsweep_block(NS);
+    long long nb = (nface - 1 + XB - 2) / (XB - 1);   // CTA b covers faces (XB-1) b .. (XB-1) b + XB-1
     if (nb > 0x7fffffffLL) return STX_E_INVALID;
-    k_euler_x<NS><<<(unsigned)nb, 128, 0, s>>>(c, wa, fl, nmin, nmax, ow);
+    k_euler_x<NS, R><<<(unsigned)nb, XB, 0, s>>>(c, cg, wa, fl, nmin, nmax, ow);
   } else {
     int ncell = nmax - nmin + 1;
     dim3 grid((g.nx + YZ_TI - 1) / YZ_TI, dir == 1 ? g.nz : g.ny, (ncell + YZ_TF - 2) / (YZ_TF - 1));
     dim3 block(YZ_TI, YZ_TF);
-    if (dir == 1) k_euler_yz<NS, 1><<<grid, block, 0, s>>>(c, wa, fl, nmin, nmax, ow);
-    else k_euler_yz<NS, 2><<<grid, block, 0, s>>>(c, wa, fl, nmin, nmax, ow);
+    if (dir == 1) k_euler_yz<NS, 1, R><<<grid, block, 0, s>>>(c, cg, wa, fl, nmin, nmax, ow);
+    else k_euler_yz<NS, 2, R><<<grid, block, 0, s>>>(c, cg, wa, fl, nmin, nmax, ow);
   }
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
 
-int launch_euler(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl, int nmin, int nmax, int ow) {
+// the plain form computes the central faces in FP64, the mixed form in FP32
+template <int NS>
+static int euler_t(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
+                   int nmax, int ow) {
+  return c.p.mixed ? euler_r<NS, float>(c, cg, s, dir, wa, fl, nmin, nmax, ow)
+                   : euler_r<NS, double>(c, cg, s, dir, wa, fl, nmin, nmax, ow);
+}
+
+int launch_euler(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
+                 int nmax, int ow) {
   switch (c.t.ns) {
-#define X(N) case N: return euler_t<N>(c, s, dir, wa, fl, nmin, nmax, ow);
+#define X(N) case N: return euler_t<N>(c, cg, s, dir, wa, fl, nmin, nmax, ow);
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;

@@ -14,7 +14,9 @@ int launch_update_field(const DevCtx &c, cudaStream_t s, double *w, const double
                         const int32_t *mask, double gamdt, int fused);
 int launch_compute_dt(const DevCtx &c, cudaStream_t s, const double *wa, const int32_t *mask, unsigned long long *out9);
 
-int launch_euler(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl, int nmin, int nmax, int overwrite);
+// cg: a device-resident copy of c, for the out-of-line WENO face fluxes
+int launch_euler(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
+                 int nmax, int overwrite);
 int launch_visflx(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl);
 int launch_visflx_reduced(const DevCtx &c, cudaStream_t s, const double *wa, double *fl);
 

@@ -8,61 +8,63 @@
 // face flux -- and the species enthalpies of the shared point -- in registers.
 #include "stx_kernels.cuh"
 
-// One staggered face between points p (left) and q = p + st (right); xl, xr
-// are the coordinates of the two points.  hl carries the species enthalpies at
+// One staggered face between points p (left) and q = p + st (right), computed in
+// R (double: plain form; float: mixed form, fields rounded once on load).  hl
+// carries the species enthalpies at
 // the left point in and those of the right point out (reused by the next face).
-template <int NS>
+template <int NS, typename R>
 __device__ __forceinline__ void visc_face(const DevCtx &c, const double *__restrict__ wa, long long p, long long q,
-                                          double dxf, double *hl, bool have_hl, double *fh) {
+                                          R dxf, R *hl, bool have_hl, R *fh) {
   const DevGrid &g = c.g;
   const DevTab &t = c.t;
+  auto ld = [&](long long r, int m) -> R { return (R)FG(wa, r, m); };
   const int J_U = NS + 1, J_V = NS + 2, J_W = NS + 3, J_T = NS + 5, J_MU = NS + 8, J_K = NS + 13, J_D = NS + 13;
-  double uu = FG(wa, p, J_U), uup = FG(wa, q, J_U), vv = FG(wa, p, J_V), vvp = FG(wa, q, J_V);
-  double ww = FG(wa, p, J_W), wwp = FG(wa, q, J_W), tt = FG(wa, p, J_T), ttp = FG(wa, q, J_T);
-  double mu = FG(wa, p, J_MU), mup = FG(wa, q, J_MU), kc = FG(wa, p, J_K), kcp = FG(wa, q, J_K);
-  double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-  double qqp = 0.5 * (uup * uup + vvp * vvp + wwp * wwp);
-  double sigx = uup - uu, sigy = vvp - vv, sigz = wwp - ww;
-  double sigq_tt = ttp - tt, sigq_qq = qqp - qq;
-  double muf = mu + mup;
-  muf = 0.5 * muf / dxf;
-  double kf = kc + kcp;
-  kf = 0.5 * kf / dxf;
+  R uu = ld(p, J_U), uup = ld(q, J_U), vv = ld(p, J_V), vvp = ld(q, J_V);
+  R ww = ld(p, J_W), wwp = ld(q, J_W), tt = ld(p, J_T), ttp = ld(q, J_T);
+  R mu = ld(p, J_MU), mup = ld(q, J_MU), kc = ld(p, J_K), kcp = ld(q, J_K);
+  R qq = R(0.5) * (uu * uu + vv * vv + ww * ww);
+  R qqp = R(0.5) * (uup * uup + vvp * vvp + wwp * wwp);
+  R sigx = uup - uu, sigy = vvp - vv, sigz = wwp - ww;
+  R sigq_tt = ttp - tt, sigq_qq = qqp - qq;
+  R muf = mu + mup;
+  muf = R(0.5) * muf / dxf;
+  R kf = kc + kcp;
+  kf = R(0.5) * kf / dxf;
   sigx = sigx * muf; sigy = sigy * muf; sigz = sigz * muf;
-  double sigq = sigq_tt * kf + sigq_qq * muf;
-  double yl[NS], yp[NS];
+  R sigq = sigq_tt * kf + sigq_qq * muf;
+  R yl[NS], yp[NS];
 #pragma unroll
-  for (int k = 0; k < NS; k++) { yl[k] = FG(wa, p, k + 1); yp[k] = FG(wa, q, k + 1); }
-  double rm = ldg(t.rgas) * yl[0];
+  for (int k = 0; k < NS; k++) { yl[k] = ld(p, k + 1); yp[k] = ld(q, k + 1); }
+  R rm = (R)ldg(t.rgas) * yl[0];
 #pragma unroll
-  for (int k = 1; k < NS; k++) rm = rm + ldg(t.rgas + k) * yl[k];
-  double mwm = t.Ru / rm;
-  rm = ldg(t.rgas) * yp[0];
+  for (int k = 1; k < NS; k++) rm = rm + (R)ldg(t.rgas + k) * yl[k];
+  R mwm = R(t.Ru) / rm;
+  rm = (R)ldg(t.rgas) * yp[0];
 #pragma unroll
-  for (int k = 1; k < NS; k++) rm = rm + ldg(t.rgas + k) * yp[k];
-  double mwmp = t.Ru / rm;
-  double mwmif = 0.5 * (mwmp + mwm) / (mwmp * mwm);
+  for (int k = 1; k < NS; k++) rm = rm + (R)ldg(t.rgas + k) * yp[k];
+  R mwmp = R(t.Ru) / rm;
+  R mwmif = R(0.5) * (mwmp + mwm) / (mwmp * mwm);
   mwmif = mwmif / dxf;
-  double rd[NS];
-  double fhat_tmp = 0.0;
+  R rd[NS];
+  R fhat_tmp = R(0.0);
 #pragma unroll
   for (int k = 0; k < NS; k++) {
-    rd[k] = 0.5 * (FG(wa, p, J_D + 1 + k) + FG(wa, q, J_D + 1 + k));
-    double xxp = yp[k] * mwmp, xx = yl[k] * mwm;
+    rd[k] = R(0.5) * (ld(p, J_D + 1 + k) + ld(q, J_D + 1 + k));
+    R xxp = yp[k] * mwmp, xx = yl[k] * mwm;
     fhat_tmp = fhat_tmp + (xxp - xx) * rd[k];
   }
   fhat_tmp = fhat_tmp * mwmif;
-  double et = 0.0;
+  R et = R(0.0);
 #pragma unroll
   for (int k = 0; k < NS; k++) {
-    double yyf = 0.5 * (yp[k] + yl[k]);
-    double xxp = yp[k] * mwmp, xx = yl[k] * mwm;
-    double sig = -rd[k] * (xxp - xx) * mwmif + fhat_tmp * yyf;
+    R yyf = R(0.5) * (yp[k] + yl[k]);
+    R xxp = yp[k] * mwmp, xx = yl[k] * mwm;
+    R sig = -rd[k] * (xxp - xx) * mwmif + fhat_tmp * yyf;
     fh[k] = sig;
-    double hh = have_hl ? hl[k] : species_poly_int(t, t.cp, tt, k + 1);
-    double hhp = species_poly_int(t, t.cp, ttp, k + 1);
+    R hh = have_hl ? hl[k] : (R)species_poly_int(t, t.cp, (double)tt, k + 1);
+    R hhp = (R)species_poly_int(t, t.cp, (double)ttp, k + 1);
     hl[k] = hhp;
-    double hhf = 0.5 * (hh + hhp);
+    R hhf = R(0.5) * (hh + hhp);
     et = et + sig * hhf;
   }
   fh[NS] = -sigx;
@@ -71,34 +73,44 @@ __device__ __forceinline__ void visc_face(const DevCtx &c, const double *__restr
   fh[NS + 3] = -sigq + et;
 }
 
-template <int NS>
+// x sweep: the faces 0..nx of every (j, k) row are numbered as one sequence
+// F = row * (nx + 1) + f; CTA b of XB threads computes faces (XB-1) b ..
+// (XB-1) b + XB-1 (one shared with the next CTA) into shared memory, and the
+// threads whose face is not the first of its row form the divergence -- every
+// thread busy for any nx.
+template <int NS, typename R>
 __global__ void __launch_bounds__(128) k_visc_x(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
-  __shared__ double sf[NV][128];
-  int j = blockIdx.y + 1, k = blockIdx.z + 1;
-  int f0 = blockIdx.x * 127;            // faces 0..nx
-  int f = f0 + threadIdx.x;
+  constexpr int XB = xsweep_block(NS);
+  __shared__ R sf[NV][XB];
+  const long long nf = g.nx + 1;
+  const long long F = (long long)blockIdx.x * (XB - 1) + threadIdx.x;
+  const bool act = F < nf * g.ny * g.nz;
+  const long long row = F / nf;
+  const int f = (int)(F - row * nf);
+  const int j = 1 + (int)(row % g.ny), k = 1 + (int)(row / g.ny);
 #define XC(i) ldg(g.x + (i) + g.ng - 1)
-  if (f <= g.nx) {
-    double fh[NV], hl[NS];
+  if (act) {
+    R fh[NV], hl[NS];
     long long p = gidx(g, f, j, k);
-    visc_face<NS>(c, wa, p, p + 1, XC(f + 1) - XC(f), hl, false, fh);
+    visc_face<NS, R>(c, wa, p, p + 1, (R)(XC(f + 1) - XC(f)), hl, false, fh);
 #pragma unroll
     for (int m = 0; m < NV; m++) sf[m][threadIdx.x] = fh[m];
   }
   __syncthreads();
   int i = f;
-  if (threadIdx.x >= 1 && i <= g.nx) {
+  if (threadIdx.x >= 1 && act && i >= 1) {
     long long q = fidx(g, i, j, k);
     double dxhl = 2.0 / (XC(i + 1) - XC(i - 1));
 #pragma unroll
-    for (int m = 0; m < NV; m++) FI(fl, q, m + 1) = FI(fl, q, m + 1) + dxhl * (sf[m][threadIdx.x] - sf[m][threadIdx.x - 1]);
+    for (int m = 0; m < NV; m++)
+      FI(fl, q, m + 1) = FI(fl, q, m + 1) + (double)((R)dxhl * (sf[m][threadIdx.x] - sf[m][threadIdx.x - 1]));
   }
 #undef XC
 }
 
-template <int NS, int DIR>
+template <int NS, int DIR, typename R>
 __global__ void __launch_bounds__(128) k_visc_yz(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl, int chunk) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
@@ -111,20 +123,20 @@ __global__ void __launch_bounds__(128) k_visc_yz(DevCtx c, const double *__restr
   long long st = DIR == 1 ? (long long)g.nxg : (long long)g.nxg * g.nyg;
   const double *xc = DIR == 1 ? g.y : g.z;
 #define XC(i) ldg(xc + (i) + g.ng - 1)
-  double prev[NV], cur[NV], hl[NS];
+  R prev[NV], cur[NV], hl[NS];
   {
     int f = c0 - 1;
     long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
-    visc_face<NS>(c, wa, p, p + st, XC(f + 1) - XC(f), hl, false, prev);
+    visc_face<NS, R>(c, wa, p, p + st, (R)(XC(f + 1) - XC(f)), hl, false, prev);
   }
   for (int f = c0; f <= c1; f++) {
     long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
-    visc_face<NS>(c, wa, p, p + st, XC(f + 1) - XC(f), hl, true, cur);
+    visc_face<NS, R>(c, wa, p, p + st, (R)(XC(f + 1) - XC(f)), hl, true, cur);
     long long q = DIR == 1 ? fidx(g, i, f, tr) : fidx(g, i, tr, f);
     double dxhl = 2.0 / (XC(f + 1) - XC(f - 1));
 #pragma unroll
     for (int m = 0; m < NV; m++) {
-      FI(fl, q, m + 1) = FI(fl, q, m + 1) + dxhl * (cur[m] - prev[m]);
+      FI(fl, q, m + 1) = FI(fl, q, m + 1) + (double)((R)dxhl * (cur[m] - prev[m]));
       prev[m] = cur[m];
     }
   }
@@ -176,21 +188,30 @@ __global__ void __launch_bounds__(256) k_visc_reduced(DevCtx c, const double *__
   FI(fl, tid, ns + 4) = FI(fl, tid, ns + 4) - sigq;
 }
 
-template <int NS>
-static int visc_t(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl) {
+template <int NS, typename R>
+static int visc_r(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl) {
   const DevGrid &g = c.g;
   if (dir == 0) {
-    dim3 grid((g.nx + 1 + 126) / 127, g.ny, g.nz);
-    k_visc_x<NS><<<grid, 128, 0, s>>>(c, wa, fl);
+    constexpr int XB = xsweep_block(NS);
+    long long nface = (long long)(g.nx + 1) * g.ny * g.nz;
+    long long nb = (nface - 1 + XB - 2) / (XB - 1);
+    if (nb > 0x7fffffffLL) return STX_E_INVALID;
+    k_visc_x<NS, R><<<(unsigned)nb, XB, 0, s>>>(c, wa, fl);
   } else {
-    int chunk = 16;
+    int chunk = 8;
     int n = dir == 1 ? g.ny : g.nz;
     dim3 grid((g.nx + 127) / 128, dir == 1 ? g.nz : g.ny, (n + chunk - 1) / chunk);
-    if (dir == 1) k_visc_yz<NS, 1><<<grid, 128, 0, s>>>(c, wa, fl, chunk);
-    else k_visc_yz<NS, 2><<<grid, 128, 0, s>>>(c, wa, fl, chunk);
+    if (dir == 1) k_visc_yz<NS, 1, R><<<grid, 128, 0, s>>>(c, wa, fl, chunk);
+    else k_visc_yz<NS, 2, R><<<grid, 128, 0, s>>>(c, wa, fl, chunk);
   }
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
+}
+
+// the plain form in FP64, the mixed form in FP32 (accumulated into the FP64 residual)
+template <int NS>
+static int visc_t(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl) {
+  return c.p.mixed ? visc_r<NS, float>(c, s, dir, wa, fl) : visc_r<NS, double>(c, s, dir, wa, fl);
 }
 
 int launch_visflx(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl) {

@@ -157,6 +157,143 @@ def turbulence_fields(c, seed: int, xp=np, device=None):
     return W, WA
 
 
+# The reactive shock tube's inputs (examples/reactive_shock_tube/multideal.ini):
+# H2:O2:Ar = 2:1:7 by moles, reflecting wall at xmin, extrapolation at xmax,
+# WENO5 everywhere (threshold -0.2), Strang + ROK4, fixed dt 2e-8 s.
+TUBE_INI = {
+    "ref_state": {"rho0": "0.072", "p0": "7173.", "u0": "0.", "init_Y_01": "0.01267282566",
+                  "init_Y_02": "0.10138260528", "init_Y_03": "0.", "init_Y_04": "0.", "init_Y_05": "0.",
+                  "init_Y_06": "0.", "init_Y_07": "0.", "init_Y_08": "0.", "init_Y_09": "0.88594456906"},
+    "grid": {"domain_size_x": "0.12", "domain_size_y": "0.01", "domain_size_z": "0.01", "nymax": "1",
+             "nzmax": "1", "ng": "3", "metrics_order": "6", "grid_type": "2"},
+    "bc": {"xmin": "8", "xmax": "2", "ymin": "0", "ymax": "0", "zmin": "0", "zmax": "0", "xmin_nr": "0",
+           "xmax_nr": "0", "ymin_nr": "0", "ymax_nr": "0", "zmin_nr": "0", "zmax_nr": "0"},
+    "controls": {"cfl": "-2E-8", "iter_dt_recompute": "1", "num_iter": "1"},
+    "numerics": {"ep_order": "6", "nkeep": "0", "visc_order": "6", "conservative_viscous": "1", "weno_scheme": "3",
+                 "weno_version": "1", "flux_splitting": "0", "sensor_threshold": "-0.2", "sensor_type": "0",
+                 "rk_type": "1", "ros_dttry": "1.e-9", "ros_eps": "1.e-8", "ros_maxsteps": "10000",
+                 "ros_maxtry": "40", "operator_splitting": "2", "rosenbrock_version": "2"},
+    "flow": {"flow_init": "9"},
+    "fluid": {"use_cantera": "1", "enable_chemistry": "2", "t_min_tab": "200.", "t_max_tab": "20000.",
+              "dt_tab": "1."},
+}
+
+
+def tube_case(nx: int, ny: int = 1, tables: M.Tables = None):
+    """The reactive shock tube on nx x ny cells (ny > 1: the same 1-D state on a
+    2-D periodic-in-y strip of height 0.01 m * ny / 128)."""
+    cfg = CS.Config()
+    for sec, kv in TUBE_INI.items():
+        for k, v in kv.items():
+            cfg.set(sec, k, v)
+    cfg.set("grid", "nxmax", nx)
+    cfg.set("grid", "nymax", ny)
+    if ny > 1:
+        cfg.set("grid", "domain_size_y", repr(0.01 * ny / 128.0))
+    if tables is None:
+        tables = M.build_tables(mechanism("shock_tube_9sp"), 7173.0, 200.0, 20000.0, 1.0)
+    return CS.Case(cfg, tables)
+
+
+def flame_case(nx: int, phi: float = 0.6, Tu: float = 298.0, tables: M.Tables = None, L: float = 0.03,
+               delta: float = 3e-4, mech_name: str = "flame_11sp"):
+    """A 1-D laminar premixed H2/air flame on nx cells of an L-long domain: the
+    settings of examples/laminar_premix_flame (11 species by default, or the
+    9-species H2/air mechanism with mech_name="h2air_9sp"; inflow at xmin,
+    extrapolation at xmax, WENO5-Z everywhere with KEEP(2), "simpler" splitting
+    with ROK4, fixed dt 1e-8 s).  The reference reads its profile from
+    premix.dat; here a synthetic flame of the same shape stands in: T, Y blend
+    between the unburnt mixture (equivalence ratio phi, Tu, 1 atm) and its
+    complete-combustion products at the adiabatic temperature through a tanh of
+    thickness delta at L/2, with constant mass flux rho u."""
+    mech = mechanism(mech_name)
+    if tables is None:
+        tables = M.build_tables(mech, 101325.0, 200.0, 5500.0, 1.0)
+    ns = mech.ns
+    iH2, iO2, iH2O, iN2 = mech.index("H2"), mech.index("O2"), mech.index("H2O"), mech.index("N2")
+    mw = np.array([s.mw for s in mech.species])
+    X = np.zeros(ns)
+    X[iH2], X[iO2], X[iN2] = 2.0 * phi, 1.0, 3.76
+    Yu = X * mw / np.dot(X, mw)
+    # complete combustion 2 H2 + O2 -> 2 H2O (per unit mass of mixture)
+    nH2, nO2 = Yu[iH2] / mw[iH2], Yu[iO2] / mw[iO2]
+    burn = min(nH2, 2.0 * nO2)
+    Yb = Yu.copy()
+    Yb[iH2] -= burn * mw[iH2]
+    Yb[iO2] -= 0.5 * burn * mw[iO2]
+    Yb[iH2O] += burn * mw[iH2O]
+    Yb = np.maximum(Yb, 0.0)
+    Yb /= Yb.sum()
+    hu = M.mixture_h(tables, Tu, Yu)
+    Tb = 2000.0
+    for _ in range(50):           # adiabatic T of the products (constant p): h(Tb, Yb) = h(Tu, Yu)
+        f = M.mixture_h(tables, Tb, Yb) - hu
+        Tb -= f / M.mixture_cp(tables, Tb, Yb)
+        if abs(f) < 1e-9 * abs(hu) + 1e-6:
+            break
+    p0 = 101325.0
+    rho_u = p0 / (np.dot(tables.rgas, Yu) * Tu)
+    su = 0.9139672490375892        # inflow speed of the reference's flame case
+    cfg = CS.default_ini(nx, 1, 1, L=(L, 1.0, 1.0), bc=(1, 2, 0, 0, 0, 0), t0=Tu, p0=p0, Y=Yu, ns=ns,
+                         chemistry=2, rosenbrock_version=2, splitting=1, weno_version=1, sensor_threshold=-0.2,
+                         sensor_type=0, nkeep=2, ep_order=6, flux_splitting=0, cfl=-1e-8, flow_init=100)
+    cfg.set("ref_state", "u0", repr(su))
+    c = CS.Case(cfg, tables)
+    ng = c.ng
+    x = c.x[ng:ng + nx]
+    s = 0.5 * (1.0 + np.tanh((x - 0.5 * L) / delta))
+    T = (1.0 - s) * Tu + s * Tb
+    Y = (1.0 - s)[None, :] * Yu[:, None] + s[None, :] * Yb[:, None]
+    rho = p0 / (np.einsum("k,kx->x", tables.rgas, Y) * T)
+    u = rho_u * su / rho
+    sh = (1, 1, nx)
+    c.set_interior(rho.reshape(sh), u.reshape(sh), np.zeros(sh), np.zeros(sh), T.reshape(sh),
+                   Y.reshape((ns,) + sh))
+    c.flame = dict(phi=phi, Tu=Tu, Tb=Tb, Yu=Yu, Yb=Yb)
+    return c
+
+
+def stiff_mechanism_tables(seed: int = 0):
+    mech = M.synthetic_mechanism(53, 325, seed)
+    return mech, M.build_tables(mech, 101325.0, 200.0, 5500.0, 1.0)
+
+
+def stiff_case(n: int, seed: int = 0, tables: M.Tables = None, dt: float = 1e-9, rosenbrock_version: int = 1):
+    """The stiff-mechanism scaling workload on an n^3 periodic box (side
+    2 pi mm n/128): 53 species / 325 reactions (stx.mech.synthetic_mechanism),
+    p = 1 atm, Y ~ Dirichlet(0.5) per cell and T on a smooth random field in
+    1200..2000 K (both seeded), at rest; WENO5-Z / KEEP(2) hybrid (threshold 0.1),
+    Strang splitting with the full-Jacobian Rosenbrock (rosenbrock_version 1: the
+    dense (ns+4)^2 Jacobian; the 4-vector Krylov basis of ROK4 cannot follow 53
+    stiff modes and caps its step count), fixed dt."""
+    if tables is None:
+        _, tables = stiff_mechanism_tables(seed)
+    ns = tables.ns
+    rng = np.random.default_rng(seed + 1)
+    L = 2.0 * math.pi * 1e-3 * n / 128.0
+    cfg = CS.default_ini(n, n, n, L=(L, L, L), bc=(0,) * 6, t0=1600.0, p0=101325.0, Y=np.full(ns, 1.0 / ns), ns=ns,
+                         chemistry=2, rosenbrock_version=rosenbrock_version, splitting=2, weno_version=1,
+                         sensor_threshold=0.1, sensor_type=1, nkeep=2, ep_order=6, flux_splitting=0, cfl=-dt,
+                         flow_init=100)
+    c = CS.Case(cfg, tables)
+    # smooth T: a few seeded Fourier modes, scaled to [-1, 1]
+    x = (np.arange(n) + 0.5) / n * 2.0 * math.pi
+    X, Yg, Z = np.meshgrid(x, x, x, indexing="ij")
+    f = np.zeros((n, n, n))
+    for _ in range(6):
+        k = rng.integers(1, 4, size=3)
+        ph = rng.uniform(0, 2 * math.pi, size=3)
+        f += np.sin(k[0] * X + ph[0]) * np.sin(k[1] * Yg + ph[1]) * np.sin(k[2] * Z + ph[2])
+    f = f / np.abs(f).max()
+    T = (1600.0 + 400.0 * f).transpose(2, 1, 0)            # (nz, ny, nx)
+    Yc = rng.dirichlet(np.full(ns, 0.5), size=(n, n, n))   # (nz, ny, nx, ns)
+    Yc = np.moveaxis(Yc, -1, 0)
+    rho = 101325.0 / (np.einsum("k,kzyx->zyx", tables.rgas, Yc) * T)
+    zero = np.zeros_like(T)
+    c.set_interior(rho, zero, zero, zero, T, Yc)
+    return c
+
+
 def shock_tube_case(nx: int, cfg_keys: dict, mech_name="shock_tube_9sp"):
     cfg = CS.Config()
     for sec, kv in cfg_keys.items():

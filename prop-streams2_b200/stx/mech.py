@@ -276,6 +276,53 @@ def restrict_species(mech: Mechanism, keep: Sequence[str], rename: Optional[Dict
 
 
 # --------------------------------------------------------------------------- thermo
+def synthetic_mechanism(ns: int = 53, nr: int = 325, seed: int = 0, base: Optional[Species] = None,
+                        third_body_frac: float = 0.2) -> Mechanism:
+    """The seeded stiff-mechanism workload (no counterpart in the reference,
+    which compiles N_S into its kernels, index_define.h): ns species S00.. whose
+    NASA-7 coefficients and transport parameters are those of `base` (N2 by
+    default) each scaled by U(0.95, 1.05); one molecular weight for all, so that
+    every reaction A + B <=> C + D between four distinct random species conserves
+    mass; nr reversible reactions with A ~ logU(1e8, 1e16) cm^3/mol/s (cm^6/mol^2/s
+    for the third_body_frac of three-body reactions, whose collision efficiencies
+    are U(0.5, 5) per species), b ~ U(-1.5, 2), Ea ~ U(0, 50) kcal/mol."""
+    rng = np.random.default_rng(seed)
+    if base is None:
+        base = Species("N2", {"N": 2}, 28.014, "NASA7", [200.0, 1000.0, 5000.0],
+                       [[3.298677, 0.0014082404, -3.963222e-06, 5.641515e-09, -2.444854e-12, -1020.8999, 3.950372],
+                        [2.92664, 0.0014879768, -5.68476e-07, 1.0097038e-10, -6.753351e-15, -922.7977, 5.980528]],
+                       geometry=1, well_depth=97.53, diameter=3.621, polarizability=1.76, rot_relax=4.0)
+    species = []
+    for k in range(ns):
+        f = lambda: float(rng.uniform(0.95, 1.05))
+        coeffs = [[c * f() for c in rng_coeffs] for rng_coeffs in base.coeffs]
+        species.append(Species(f"S{k:02d}", dict(base.composition), base.mw, "NASA7", list(base.tranges), coeffs,
+                               geometry=base.geometry, well_depth=base.well_depth * f(),
+                               diameter=base.diameter * f(), dipole=base.dipole,
+                               polarizability=base.polarizability * f(), rot_relax=base.rot_relax))
+    names = [s.name for s in species]
+    reactions = []
+    cal = 4.184e6                              # kcal/mol -> J/kmol
+    for _ in range(nr):
+        a, b, c, d = rng.choice(ns, size=4, replace=False)
+        reac = {names[a]: 1.0, names[b]: 1.0}
+        prod = {names[c]: 1.0, names[d]: 1.0}
+        third = rng.uniform() < third_body_frac
+        A = 10.0 ** rng.uniform(8.0, 16.0)
+        bexp = float(rng.uniform(-1.5, 2.0))
+        Ea = float(rng.uniform(0.0, 50.0)) * cal
+        if third:
+            A *= (1e-6 / 1e-3) ** 2               # cm^6/mol^2/s -> m^6/kmol^2/s
+            eff = {n: float(rng.uniform(0.5, 5.0)) for n in names}
+            eq = f"{names[a]} + {names[b]} + M <=> {names[c]} + {names[d]} + M"
+            reactions.append(Reaction(eq, reac, prod, True, RT_THREEBODY, [A, bexp, Ea], efficiencies=eff))
+        else:
+            A *= 1e-6 / 1e-3                       # cm^3/mol/s -> m^3/kmol/s
+            eq = f"{names[a]} + {names[b]} <=> {names[c]} + {names[d]}"
+            reactions.append(Reaction(eq, reac, prod, True, RT_ARRHENIUS, [A, bexp, Ea]))
+    return Mechanism(species, reactions)
+
+
 def _nasa_eval(sp: Species, T: float):
     """Return (cp/R, h/RT, s/R) for one species at T (range picked like Cantera:
     the low range below the midpoint, the high range at or above it)."""

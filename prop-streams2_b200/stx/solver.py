@@ -64,15 +64,48 @@ class Solver:
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 
     def close(self):
+        for g in getattr(self, "_graphs", []):
+            self.lib.stx_graph_destroy(g)
+        self._graphs = []
         if getattr(self, "ctx", None):
             self.lib.stx_ctx_destroy(self.ctx)
             self.ctx = None
+
+    # ------------------------------------------------------------------ captured steps
+    def capture(self, nsteps: int):
+        """Capture nsteps iterations of the integration loop into one CUDA graph
+        (fixed dt only: cfl < 0, iter_dt_recompute = 1).  Replaying it with
+        ``replay`` gives the same result as nsteps calls of ``step``."""
+        if self.case.cfl >= 0 or self.case.iter_dt_recompute != 1:
+            raise ValueError("captured steps need a fixed dt (cfl < 0) and iter_dt_recompute = 1")
+        self.dt = -self.case.cfl
+        g = C.c_void_p()
+        check(self.lib.stx_graph_create(self.ctx, C.byref(self.fields), self.dt, nsteps, C.byref(g)),
+              "stx_graph_create")
+        if not hasattr(self, "_graphs"):
+            self._graphs = []
+        self._graphs.append(g)
+        return g, nsteps
+
+    def replay(self, graph):
+        g, n = graph
+        check(self.lib.stx_graph_launch(g, self.stream, self.time), "stx_graph_launch")
+        for _ in range(n):
+            self.icyc += 1
+            self.time = self.time + self.dt
 
     def __del__(self):
         try:
             self.close()
         except Exception:
             pass
+
+    def set_precision(self, form: str):
+        """"fp64" (the reference method, default) or "mixed" (FP32 face fluxes and
+        transport properties, FP64 residual, Newton and chemistry)."""
+        mode = {"fp64": 0, "mixed": 1}[form]
+        check(self.lib.stx_set_precision(self.ctx, mode), "stx_set_precision")
+        self.precision = form
 
     def aux_slot(self, j: int) -> C.c_void_p:
         return C.c_void_p(self.w_aux[j].data_ptr())
