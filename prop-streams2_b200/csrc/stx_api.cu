@@ -21,6 +21,11 @@ struct stx_ctx {
   double *time_d;                 // simulation time of captured steps (stx_graph_*)
   const DevCtx *dctx_d;           // device copy of d, for device functions that take the context by reference
   std::vector<void *> allocs;
+  // The context's own non-blocking stream: its tables and scratch are allocated,
+  // uploaded and freed stream-ordered on it (cudaMallocAsync / cudaFreeAsync), so
+  // creating or destroying a context never waits for other work on the device
+  // (a plain cudaFree synchronises the whole device).
+  cudaStream_t cs = nullptr;
   int device;
   // instrumentation (stx_profile_*)
   int prof_on;
@@ -68,10 +73,11 @@ template <typename T>
 int upload(stx_ctx *c, const T *host, size_t n, const T **out) {
   void *p = nullptr;
   if (n == 0) n = 1;
-  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return STX_E_NOMEM;
+  if (cudaMallocAsync(&p, n * sizeof(T), c->cs) != cudaSuccess) return STX_E_NOMEM;
   c->allocs.push_back(p);
-  if (host && cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return STX_E_CUDA;
-  if (!host && cudaMemset(p, 0, n * sizeof(T)) != cudaSuccess) return STX_E_CUDA;
+  // pageable host source: the copy is staged before the call returns
+  if (host && cudaMemcpyAsync(p, host, n * sizeof(T), cudaMemcpyHostToDevice, c->cs) != cudaSuccess) return STX_E_CUDA;
+  if (!host && cudaMemsetAsync(p, 0, n * sizeof(T), c->cs) != cudaSuccess) return STX_E_CUDA;
   *out = (const T *)p;
   return STX_OK;
 }
@@ -111,7 +117,13 @@ const char *stx_strerror(int code) {
 
 int stx_ctx_destroy(stx_ctx *c) {
   if (!c) return STX_E_INVALID;
-  for (void *p : c->allocs) cudaFree(p);
+  // stream-ordered frees on the context's stream: the caller has finished its
+  // work on the context's fields (its own streams are synchronised)
+  for (void *p : c->allocs) cudaFreeAsync(p, c->cs);
+  if (c->cs) {
+    cudaStreamSynchronize(c->cs);
+    cudaStreamDestroy(c->cs);
+  }
   for (int k = 0; k < STX_NK; k++)
     for (cudaEvent_t e : c->ev[k]) cudaEventDestroy(e);
   delete c;
@@ -145,6 +157,10 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   stx_ctx *c = new (std::nothrow) stx_ctx();
   if (!c) return STX_E_NOMEM;
   cudaGetDevice(&c->device);
+  if (cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return STX_E_CUDA;
+  }
   c->par = *par;
   c->ns = ns;
   c->nv = ns + 4;
@@ -227,6 +243,22 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
       if ((rc = upload(c, cnt.data(), cnt.size(), &t.sp_cnt))) return fail(rc);
       if ((rc = upload(c, idx.data(), idx.size(), &t.sp_idx))) return fail(rc);
       if ((rc = upload(c, coef.data(), coef.size(), &t.sp_coef))) return fail(rc);
+      // by species: the reactions a species takes part in (rr or pp nonzero), ascending
+      std::vector<int> kptr(ns + 1, 0), kr;
+      std::vector<double> kc;
+      for (int k = 0; k < ns; k++) {
+        for (int r = 0; r < nr; r++) {
+          double rr = tab->r_coeffs[(size_t)k * nr + r], pp = tab->p_coeffs[(size_t)k * nr + r];
+          if (rr != 0.0 || pp != 0.0) {
+            kr.push_back(r);
+            kc.push_back(pp - rr);
+          }
+        }
+        kptr[k + 1] = (int)kr.size();
+      }
+      if ((rc = upload(c, kptr.data(), kptr.size(), &t.sk_ptr))) return fail(rc);
+      if ((rc = upload(c, kr.data(), kr.size(), &t.sk_r))) return fail(rc);
+      if ((rc = upload(c, kc.data(), kc.size(), &t.sk_c))) return fail(rc);
     }
     std::vector<double> kr(ntab1 * nr);
     for (size_t it = 0; it < ntab1; it++)
@@ -290,6 +322,7 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   }
   c->par.winf = nullptr;
   if ((rc = upload<DevCtx>(c, &c->d, 1, &c->dctx_d))) return fail(rc);
+  if (cudaStreamSynchronize(c->cs) != cudaSuccess) return fail(STX_E_CUDA);
   *out = c;
   return STX_OK;
 }
@@ -471,6 +504,16 @@ int stx_batch0d_integrate(stx_ctx *c, void *s, int n, const double *T0, const do
   DevCtx d = c->d;
   d.p.ros_maxsteps = max_steps;
   Prof pf(c, S(s), STX_K_CHEM, 1, (double)n * 8.0 * (2 * c->d.t.ns + 6));
+  // one warp per reactor where the mechanism fits (ns <= 32, nr <= 64): the
+  // launch lasts as long as its slowest reactor, and a warp integrates one
+  // reactor several times faster than a thread does; STX_BATCH0D_KERNEL=thread
+  // selects the thread-per-reactor kernel
+  const char *kind = std::getenv("STX_BATCH0D_KERNEL");
+  if (!(kind && std::strcmp(kind, "thread") == 0)) {
+    int rc = launch_batch0d_warp(d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end,
+                                 nsteps, c->counter_d);
+    if (rc != STX_E_UNSUPPORTED) return rc;
+  }
   return launch_batch0d(d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end, nsteps,
                         c->counter_d);
 }
@@ -548,7 +591,8 @@ int stx_advance_solution(stx_ctx *c, void *s, const stx_fields *f, double dt, do
 int stx_set_precision(stx_ctx *c, int mode) {
   if (!c || (mode != STX_PREC_FP64 && mode != STX_PREC_MIXED)) return STX_E_INVALID;
   c->d.p.mixed = mode;
-  STX_CUDA_TRY(cudaMemcpy((void *)c->dctx_d, &c->d, sizeof(DevCtx), cudaMemcpyHostToDevice));
+  STX_CUDA_TRY(cudaMemcpyAsync((void *)c->dctx_d, &c->d, sizeof(DevCtx), cudaMemcpyHostToDevice, c->cs));
+  STX_CUDA_TRY(cudaStreamSynchronize(c->cs));
   return STX_OK;
 }
 

@@ -4,6 +4,14 @@
 #pragma once
 #include "stx_kernels.cuh"
 
+// Linkage of the ROK4 right-hand side.  Inlined at its three call sites
+// (default) it avoids the call's register saves and halves the local-memory
+// frame (2.2 KB instead of 3.9 KB per thread); measured 10 % faster than one
+// out-of-line copy now that the production rates are compact.
+#ifndef STX_RHS_LINKAGE
+#define STX_RHS_LINKAGE __forceinline__
+#endif
+
 
 // Temperature-table position of T for K_c (kernels_gpu.F90:9259-9264).
 __device__ __forceinline__ void kc_pos(const DevTab &t, double tt, int &itt, double &dtt) {
@@ -177,15 +185,13 @@ __device__ void chem_source_sp(const DevTab &t, double tt, const double *conc, d
   }
 }
 
-// rosenbrock_krylov_rhs (kernels_gpu.F90:10794-10976), PaSR off.  Kept out of
-// line: one copy serves the Arnoldi, Jacobian-vector and stage evaluations, so
-// the ROK4 loop stays small enough for the instruction cache.  With the
+// rosenbrock_krylov_rhs (kernels_gpu.F90:10794-10976), PaSR off.  With the
 // context's tables (KCF false) the production terms run over the sparse
 // stoichiometry with per-thread rows in shared memory (launch with
 // chem_block(NS) threads); with the reference's raw tables (KCF true) over the
 // dense species loops.
 template <int NS, bool KCF = false>
-__device__ __noinline__ void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, double *rhs) {
+__device__ STX_RHS_LINKAGE void krylov_rhs(const DevCtx &c, const double *w_sav, double T_iter, double *rhs) {
   const DevTab &t = c.t;
   double Y[NS], conc[NS], wl[NS];
 #pragma unroll

@@ -43,6 +43,12 @@ struct DevTab {
   const int *sp_cnt;
   const unsigned char *sp_idx;
   const double *sp_coef;
+  // the same stoichiometry by species (CSR): for species k the reactions
+  // sk_r[sk_ptr[k] .. sk_ptr[k+1]) with nu'' - nu' != 0 or a nonzero term, in
+  // ascending order, and their coefficients sk_c = nu'' - nu'
+  const int *sk_ptr;
+  const int *sk_r;
+  const double *sk_c;
   const double *wk_a, *wk_b;      // Wilke pair factors [l][m]
   int n_eoi;
   const double *aw_eoi, *coeff_eoi, *beta0;

@@ -3,16 +3,12 @@
 // kernels of src/multideal/kernels_gpu.F90:88-2063, 2065-3295).
 //
 // B200 design:
-//  * x sweep: the faces of all rows numbered as one sequence, 128 per CTA (one
-//    shared with the next CTA); the faces go through shared memory and the
-//    threads apply fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- no fhat round
-//    trip through HBM.
+//  * x sweep: one CTA of 128 threads per pencil segment; thread t computes face
+//    f0+t, the faces go through shared memory and threads 1..127 apply
+//    fl(i) += (fhat_i - fhat_{i-1}) * dxi/dx -- no fhat round trip through HBM.
 //  * y/z sweeps: tiles of 32 contiguous i (coalesced) x 8 faces along the
 //    sweep, one face per thread, differenced through shared memory; one
 //    redundant face per 7 cells.
-//  * In every sweep the central faces are computed in place and the faces the
-//    Ducros test sends to WENO are gathered per CTA and worked through by full
-//    warps.
 //  * WENO faces use the structure of the multi-species eigenvectors
 //    (kernels_gpu.F90:2703-2984): the species block of L is identity + rank one,
 //    so every characteristic variable follows from two per-point scalars
@@ -527,34 +523,31 @@ __device__ __noinline__ void weno_rusanov_flux(const DevCtx &c, const double *__
   }
 }
 
-// Hybrid face flux (kernels_gpu.F90:88-2063): the Ducros test over the WENO
-// stencil picks the central KEEP flux or the upwind (characteristic or
-// Rusanov) WENO flux.  The sweeps evaluate the test for every face first, do
-// the central faces in place, and gather the shocked faces of the CTA into a
-// list that full warps then work through, so that a few WENO faces do not
-// stall every warp they fall in.
-template <int NS>
-__device__ __forceinline__ bool face_shocked(const DevCtx &c, const double *__restrict__ wa, long long p, long long st) {
+// Hybrid face flux: Ducros test over the WENO stencil, then central or upwind.
+template <int NS, int DIR, typename R>
+__device__ __forceinline__ void face_flux(const DevCtx &c, const DevCtx *__restrict__ cg,
+                                          const double *__restrict__ wa, long long p, long long st, int face, int nmax,
+                                          R *fh) {
   const DevGrid &g = c.g;
   const int J_DUC = NS + 9;
   const int ws = c.p.weno_scheme;
   bool shk = false;
   for (int s = -ws + 1; s <= ws; s++) shk |= (FG(wa, p + s * st, J_DUC) > c.p.sensor_threshold);
-  return shk;
-}
-
-template <int NS, int DIR, typename R>
-__device__ __forceinline__ void weno_face(const DevCtx &c, const DevCtx *__restrict__ cg,
-                                          const double *__restrict__ wa, long long p, long long st, R *fh) {
-  // The out-of-line WENO fluxes take the context by reference and write
-  // through a pointer.  They get the device-resident copy cg of the context
-  // (the by-value kernel parameter c would otherwise be copied to local memory
-  // by every thread) and their own output array.
-  double fw[NS + 4];
-  if (c.p.flux_splitting == 1) weno_rusanov_flux<NS, DIR>(*cg, wa, p, st, fw);
-  else weno_char_flux<NS, DIR>(*cg, wa, p, st, fw);
+  if (!shk) {
+    bool fz = (face == 0 && c.p.fzf[2 * DIR] == 1) || (face == nmax && c.p.fzf[2 * DIR + 1] == 1);
+    central_flux<NS, DIR, R>(c, wa, p, st, fz, fh);
+  } else {
+    // The out-of-line WENO fluxes take the context by reference and write
+    // through a pointer.  They get the device-resident copy cg of the context
+    // (the by-value kernel parameter c would otherwise be copied to local
+    // memory by every thread) and their own output array (so fh stays in
+    // registers on the central path).
+    double fw[NS + 4];
+    if (c.p.flux_splitting == 1) weno_rusanov_flux<NS, DIR>(*cg, wa, p, st, fw);
+    else weno_char_flux<NS, DIR>(*cg, wa, p, st, fw);
 #pragma unroll
-  for (int m = 0; m < NS + 4; m++) fh[m] = (R)fw[m];
+    for (int m = 0; m < NS + 4; m++) fh[m] = (R)fw[m];
+  }
 }
 
 // x sweep: the faces nmin-1..nmax of every (j, k) row are numbered as one
@@ -571,40 +564,18 @@ __global__ void __launch_bounds__(128, 4) k_euler_x(DevCtx c, const DevCtx *__re
   const int NV = NS + 4;
   constexpr int XB = xsweep_block(NS);
   __shared__ R sf[NV][XB];
-  __shared__ int wlist[XB];
-  __shared__ int nw;
-  if (threadIdx.x == 0) nw = 0;
-  __syncthreads();
   const long long nf = nmax - nmin + 2;
-  const long long ntot = nf * g.ny * g.nz;
   const long long F = (long long)blockIdx.x * (XB - 1) + threadIdx.x;
-  const bool act = F < ntot;
+  const bool act = F < nf * g.ny * g.nz;
   const long long row = F / nf;
   const int f = nmin - 1 + (int)(F - row * nf);
   const int j = 1 + (int)(row % g.ny), k = 1 + (int)(row / g.ny);
   if (act) {
-    long long p = gidx(g, f, j, k);
-    if (!face_shocked<NS>(c, wa, p, 1)) {
-      R fh[NV];
-      bool fz = (f == 0 && c.p.fzf[0] == 1) || (f == g.nx && c.p.fzf[1] == 1);
-      central_flux<NS, 0, R>(c, wa, p, 1, fz, fh);
-#pragma unroll
-      for (int m = 0; m < NV; m++) sf[m][threadIdx.x] = fh[m];
-    } else {
-      wlist[atomicAdd(&nw, 1)] = threadIdx.x;
-    }
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < nw; q += XB) {
-    const int t = wlist[q];
-    const long long Ft = (long long)blockIdx.x * (XB - 1) + t;
-    const long long rt = Ft / nf;
-    const int ft = nmin - 1 + (int)(Ft - rt * nf);
-    const long long p = gidx(g, ft, 1 + (int)(rt % g.ny), 1 + (int)(rt / g.ny));
     R fh[NV];
-    weno_face<NS, 0, R>(c, cg, wa, p, 1, fh);
+    long long p = gidx(g, f, j, k);
+    face_flux<NS, 0, R>(c, cg, wa, p, 1, f, g.nx, fh);
 #pragma unroll
-    for (int m = 0; m < NV; m++) sf[m][t] = fh[m];
+    for (int m = 0; m < NV; m++) sf[m][threadIdx.x] = fh[m];
   }
   __syncthreads();
   if (threadIdx.x >= 1 && act && f >= nmin) {
@@ -636,11 +607,7 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const DevC
   const DevGrid &g = c.g;
   const int NV = NS + 4;
   __shared__ R sf[NV][YZ_TF][YZ_TI];
-  __shared__ int wlist[YZ_TF * YZ_TI];
-  __shared__ int nw;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * YZ_TI + tx;
-  if (tid == 0) nw = 0;
-  __syncthreads();
+  const int tx = threadIdx.x, ty = threadIdx.y;
   int i = blockIdx.x * YZ_TI + tx + 1;
   int tr = blockIdx.y + 1;                 // k for the y sweep, j for the z sweep
   int f = nmin - 1 + blockIdx.z * (YZ_TF - 1) + ty;
@@ -648,26 +615,11 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const DevC
   int nsw = DIR == 1 ? g.ny : g.nz;
   bool act = i <= g.nx && f <= nmax;
   if (act) {
-    long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
-    if (!face_shocked<NS>(c, wa, p, st)) {
-      R fh[NV];
-      bool fz = (f == 0 && c.p.fzf[2 * DIR] == 1) || (f == nsw && c.p.fzf[2 * DIR + 1] == 1);
-      central_flux<NS, DIR, R>(c, wa, p, st, fz, fh);
-#pragma unroll
-      for (int m = 0; m < NV; m++) sf[m][ty][tx] = fh[m];
-    } else {
-      wlist[atomicAdd(&nw, 1)] = tid;
-    }
-  }
-  __syncthreads();
-  for (int q = tid; q < nw; q += YZ_TF * YZ_TI) {
-    const int t = wlist[q], sx = t % YZ_TI, sy = t / YZ_TI;
-    const int it = blockIdx.x * YZ_TI + sx + 1, ft = nmin - 1 + blockIdx.z * (YZ_TF - 1) + sy;
-    const long long p = DIR == 1 ? gidx(g, it, ft, tr) : gidx(g, it, tr, ft);
     R fh[NV];
-    weno_face<NS, DIR, R>(c, cg, wa, p, st, fh);
+    long long p = DIR == 1 ? gidx(g, i, f, tr) : gidx(g, i, tr, f);
+    face_flux<NS, DIR, R>(c, cg, wa, p, st, f, nsw, fh);
 #pragma unroll
-    for (int m = 0; m < NV; m++) sf[m][sy][sx] = fh[m];
+    for (int m = 0; m < NV; m++) sf[m][ty][tx] = fh[m];
   }
   __syncthreads();
   if (ty >= 1 && act) {

@@ -5,9 +5,11 @@ The reference runs one solve per process.  Here solves of different kinds and
 sizes arrive over time and share the device:
 
 * reactor requests (one adiabatic constant-pressure 0-D reactor each) are
-  coalesced: whenever the reactor lane is free, every reactor request that has
-  arrived is launched in one persistent stx_batch0d_integrate launch, so
-  requests that arrive while a batch runs join the next one;
+  coalesced: whenever one of the reactor lanes (each a context with its own
+  work counter and stream) is free, every reactor request that has arrived is
+  launched in one persistent stx_batch0d_integrate launch on it, so requests
+  that arrive while batches run start in the next free lane, concurrently
+  with the running ones;
 * grid requests (1-D flames, 2-D shock tubes; fixed dt, so no host
   synchronisation inside a step) each get their own solver context, fields in
   HBM and CUDA stream, and are admitted in arrival order while the memory
@@ -67,19 +69,21 @@ class Server:
     reactor_batch: most reactors per batched launch."""
 
     def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 32, chunk: int = 5,
-                 reactor_batch: int = 16384, t_max: float = 1e-2, max_steps: int = 20000):
+                 reactor_batch: int = 16384, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 4):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         torch.cuda.set_device(self.device)
-        self.reactors = BatchReactors("h2air_9sp", device=str(self.device))
+        rtab = M.build_tables(configs.mechanism("h2air_9sp"), 101325.0, 200.0, 5500.0, 1.0)
+        self.lanes = [BatchReactors("h2air_9sp", device=str(self.device), tables=rtab) for _ in range(reactor_lanes)]
+        self.lane_streams = [torch.cuda.Stream(self.device) for _ in range(reactor_lanes)]
+        self.reactors = self.lanes[0]
         self.tables = {
             "flame1d": M.build_tables(configs.mechanism("h2air_9sp"), 101325.0, 200.0, 5500.0, 1.0),
             "tube2d": M.build_tables(configs.mechanism("shock_tube_9sp"), 7173.0, 200.0, 20000.0, 1.0),
         }
         self.mem_budget, self.max_grid, self.chunk = mem_budget, max_grid, chunk
         self.reactor_batch, self.t_max, self.max_steps = reactor_batch, t_max, max_steps
-        self.reactor_stream = torch.cuda.Stream(self.device)
 
     # ------------------------------------------------------------------ grid solves
     def _case(self, req: Request):
@@ -124,22 +128,25 @@ class Server:
         job.sol.close()
 
     # ------------------------------------------------------------------ reactors
-    def _launch_reactors(self, reqs: List[Request], now: float):
+    def _launch_reactors(self, lane: int, reqs: List[Request], now: float):
         T0 = np.array([r.params["T0"] for r in reqs])
         p0 = np.array([r.params["p0"] for r in reqs])
         Y0 = np.stack([r.params["Y0"] for r in reqs], axis=1)
-        with torch.cuda.stream(self.reactor_stream):
-            out = self.reactors.integrate(T0, p0, Y0, self.t_max, 1e-8, 1.05, 2.0, self.max_steps, sync=False,
-                                          order="coldest_first")
+        st = self.lane_streams[lane]
+        with torch.cuda.stream(st):
+            out = self.lanes[lane].integrate(T0, p0, Y0, self.t_max, 1e-8, 1.05, 2.0, self.max_steps, sync=False,
+                                             order="coldest_first")
             ev = torch.cuda.Event()
-            ev.record(self.reactor_stream)
+            ev.record(st)
         for r in reqs:
             r.admitted = now
-        return reqs, out, ev
+        return reqs, out, ev, st
 
     def _finish_reactors(self, batch, now: float):
-        reqs, out, _ = batch
-        host = {k: v.cpu().numpy() for k, v in out.items()}
+        reqs, out, ev, st = batch
+        ev.synchronize()
+        with torch.cuda.stream(st):      # not the legacy default stream: it would wait for every lane
+            host = {k: v.cpu().numpy() for k, v in out.items()}
         for i, r in enumerate(reqs):
             r.result = {"Y": host["Y"][:, i].copy(), "T": float(host["T"][i]), "t_ign": float(host["t_ign"][i]),
                         "t_end": float(host["t_end"][i]), "nsteps": int(host["nsteps"][i])}
@@ -157,7 +164,7 @@ class Server:
         pending_r: List[Request] = []
         pending_g: List[Request] = []
         active: List[_GridJob] = []
-        batch = None
+        batches = [None] * len(self.lanes)
         mem_used = 0
         nxt = 0
         t0 = time.perf_counter()
@@ -170,16 +177,17 @@ class Server:
                 (pending_r if todo[nxt].kind == "reactor" else pending_g).append(todo[nxt])
                 nxt += 1
             progressed = False
-            # reactor lane
-            if batch is not None and batch[2].query():
-                self._finish_reactors(batch, clock())
-                n_done += len(batch[0])
-                batch = None
-                progressed = True
-            if batch is None and pending_r:
-                take, pending_r = pending_r[:self.reactor_batch], pending_r[self.reactor_batch:]
-                batch = self._launch_reactors(take, clock())
-                progressed = True
+            # reactor lanes
+            for ln in range(len(self.lanes)):
+                if batches[ln] is not None and batches[ln][2].query():
+                    self._finish_reactors(batches[ln], clock())
+                    n_done += len(batches[ln][0])
+                    batches[ln] = None
+                    progressed = True
+                if batches[ln] is None and pending_r:
+                    take, pending_r = pending_r[:self.reactor_batch], pending_r[self.reactor_batch:]
+                    batches[ln] = self._launch_reactors(ln, take, clock())
+                    progressed = True
             # grid lanes
             still = []
             for job in active:
@@ -242,7 +250,8 @@ class Server:
         return self._Shape(nv, nv_aux, nx + 2 * ng, ny + 2 * ng, 1 + 2 * ng, nx, ny, 1)
 
     def close(self):
-        self.reactors.close()
+        for br in self.lanes:
+            br.close()
 
 
 def mixed_requests(n: int, rate: float, seed: int, mech: M.Mechanism, flame_steps: int = 20,

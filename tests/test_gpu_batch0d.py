@@ -91,3 +91,19 @@ def test_batch_reactor_conserves_enthalpy_and_mass(batch):
     h1 = np.array([M.mixture_h(tb, g["T"][r], np.maximum(g["Y"][:, r], 0.0)) for r in range(T0.size)])
     assert np.max(np.abs(h1 - h0) / np.abs(h0).max()) < 1e-9
     assert np.all(g["T"] > 1.2 * T0)               # burnt (lean mixtures end cooler)
+
+
+def test_warp_and_thread_reactor_kernels_agree(batch, monkeypatch):
+    """The warp-per-reactor kernel (default where the mechanism fits) and the
+    thread-per-reactor kernel integrate the same reactors to the same answer
+    within the adaptive integration's conditioning (different summation order
+    of the Krylov dot products)."""
+    T0, p0, Y0 = sample_h2air(48, 31, batch.mech, T_range=(1100.0, 1500.0))
+    w = {k: v.cpu().numpy() for k, v in batch.integrate(T0, p0, Y0, T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS).items()}
+    monkeypatch.setenv("STX_BATCH0D_KERNEL", "thread")
+    t = {k: v.cpu().numpy() for k, v in batch.integrate(T0, p0, Y0, T_MAX, DTTRY, 1.05, 2.0, MAXSTEPS).items()}
+    ign = t["t_ign"] > 0
+    assert np.array_equal(w["t_ign"] > 0, ign)
+    r = np.abs(w["t_ign"][ign] - t["t_ign"][ign]) / t["t_ign"][ign]
+    assert r.max() < 1e-3 and np.median(r) < 1e-5, (r.max(), np.median(r))
+    assert np.max(np.abs(w["T"] - t["T"]) / t["T"]) < 1e-3
