@@ -237,8 +237,36 @@ int stx_rosenbrock_krylov_noalloc(const stx_params *par, const stx_tables *tab_d
                                   void *stream, double *w, const double *w_aux, const double *fl_sav,
                                   double dttry, double time_start, double time_end, int simpler, uint32_t *status);
 
+/* Launch choices of a context that leave the method unchanged: the candidates
+ * compute the same face fluxes and cell updates (equal up to rounding between
+ * sweep kinds; bit for bit between WENO placements and CTA counts), so a fixed
+ * tuning gives reproducible results.  No counterpart in the reference. */
+typedef struct stx_tuning {
+  int32_t sweep_kind[3];     /* convective sweep x, y, z: 0 staged shared-memory tiles, 1 one face per thread */
+  int32_t weno_list[3];      /* 1: the faces the Ducros sensor marks are listed and computed by full warps;
+                                0: computed in line by the sweep */
+  int32_t chem_ctas_per_sm;  /* persistent CTAs per SM of the cell chemistry (ROK4); 0: its occupancy limit */
+  int32_t chem_ctas_max;     /* out: that occupancy limit */
+  float sweep_ms[3];         /* out (stx_autotune): time of the chosen sweep kernels, ms */
+  float chem_ms;             /* out (stx_autotune): time of the chosen chemistry launch, ms */
+} stx_tuning;
+int stx_get_tuning(stx_ctx *ctx, stx_tuning *out);
+int stx_set_tuning(stx_ctx *ctx, const stx_tuning *t);
+/* The autotuner: times every candidate of stx_tuning on the caller's fields
+ * (f->w and f->w_aux as after compute_aux; neither is modified -- the sweeps
+ * write a scratch residual, the chemistry runs on a scratch copy of w over
+ * [0, dt_chem]), keeps the fastest in the context and returns the choice.
+ * Synchronises the stream; call it outside any stream capture. */
+int stx_autotune(stx_ctx *ctx, void *stream, const stx_fields *f, double dt_chem, stx_tuning *out);
+
 /* Device status word (OR of STX_ST_* bits since the last reset); synchronises the stream. */
 int stx_status(stx_ctx *ctx, void *stream, uint32_t *bits, int reset);
+
+/* The same read without a synchronisation: enqueues on the stream the copy of the
+ * status word into *bits (pinned host memory, or device memory) and then, if
+ * reset, its reset.  *bits holds the value once the stream has reached this
+ * point (an event recorded after the call has completed). */
+int stx_status_enqueue(stx_ctx *ctx, void *stream, uint32_t *bits, int reset);
 
 /* Instrumentation: kernel classes whose launches are counted and, while
  * profiling is on, timed with CUDA events recorded on the launching stream. */

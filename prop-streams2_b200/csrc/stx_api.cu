@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -20,11 +21,13 @@ struct stx_ctx {
   unsigned long long *dt_d;       // the nine CFL maxima
   double *time_d;                 // simulation time of captured steps (stx_graph_*)
   const DevCtx *dctx_d;           // device copy of d, for device functions that take the context by reference
+  WenoScratch weno;               // listed WENO faces of the staged sweeps (cap 0: none)
+  int weno_list[3];               // per sweep direction: use the listed WENO faces
   std::vector<void *> allocs;
   // The context's own non-blocking stream: its tables and scratch are allocated,
-  // uploaded and freed stream-ordered on it (cudaMallocAsync / cudaFreeAsync), so
-  // creating or destroying a context never waits for other work on the device
-  // (a plain cudaFree synchronises the whole device).
+  // uploaded and freed stream-ordered on it (cudaMallocFromPoolAsync /
+  // cudaFreeAsync), so creating or destroying a context never waits for other
+  // work on the device (a plain cudaFree synchronises the whole device).
   cudaStream_t cs = nullptr;
   int device;
   // instrumentation (stx_profile_*)
@@ -69,11 +72,36 @@ struct Prof {
 
 namespace {
 
+// The library's memory pool on a device, for context tables and scratch.  Its
+// release threshold is the maximum, so memory freed by a destroyed context stays
+// in the pool for the next one instead of being unmapped at the next
+// synchronisation (contexts come and go while other work runs, e.g. one per
+// served request).
+cudaMemPool_t ctx_pool(int dev) {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+  if (!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    pools[dev] = pool;
+  }
+  return pools[dev];
+}
+
 template <typename T>
 int upload(stx_ctx *c, const T *host, size_t n, const T **out) {
   void *p = nullptr;
   if (n == 0) n = 1;
-  if (cudaMallocAsync(&p, n * sizeof(T), c->cs) != cudaSuccess) return STX_E_NOMEM;
+  cudaMemPool_t pool = ctx_pool(c->device);
+  if (!pool || cudaMallocFromPoolAsync(&p, n * sizeof(T), pool, c->cs) != cudaSuccess) return STX_E_NOMEM;
   c->allocs.push_back(p);
   // pageable host source: the copy is staged before the call returns
   if (host && cudaMemcpyAsync(p, host, n * sizeof(T), cudaMemcpyHostToDevice, c->cs) != cudaSuccess) return STX_E_CUDA;
@@ -90,6 +118,20 @@ bool ns_supported(int ns) {
 }
 
 inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+// mean time of reps launches of fn on s after one untimed launch, in ms (-1 on error)
+template <class F>
+float time_launches(cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, int reps, F fn) {
+  if (fn() != STX_OK) return -1.f;
+  cudaEventRecord(e0, s);
+  for (int r = 0; r < reps; r++)
+    if (fn() != STX_OK) return -1.f;
+  cudaEventRecord(e1, s);
+  if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  return ms / reps;
+}
 
 }  // namespace
 
@@ -314,6 +356,11 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   c->dt_d = (unsigned long long *)dtp;
   c->time_d = (double *)tm;
   p.status = c->status_d;
+  {
+    const char *ek = std::getenv("STX_EULER_KERNEL");
+    int face = ek && std::strcmp(ek, "face") == 0;
+    for (int q = 0; q < 3; q++) p.sweep_kind[q] = face;
+  }
   c->winf_d = nullptr;
   if (par->winf) {
     const double *wf = nullptr;
@@ -321,6 +368,23 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
     c->winf_d = (double *)wf;
   }
   c->par.winf = nullptr;
+  if ((rc = launch_euler_setup(ns))) return fail(rc);
+  for (int q = 0; q < 3; q++) c->weno_list[q] = 1;
+  c->weno = WenoScratch{nullptr, nullptr, nullptr, 0};
+  const char *wl_env = std::getenv("STX_WENO_LIST");
+  if (ns <= 14 && !(wl_env && std::strcmp(wl_env, "0") == 0)) {
+    // the staged sweeps (ns <= 14) read the listed WENO faces' fluxes (STX_WENO_LIST=0: computed in line)
+    const long long cap = weno_scratch_faces(g);
+    const unsigned int *wc = nullptr;
+    const int *wl = nullptr;
+    const double *wf = nullptr;
+    if (cap < 0x7fffffffLL) {
+      if ((rc = upload<unsigned int>(c, nullptr, 1, &wc))) return fail(rc);
+      if ((rc = upload<int>(c, (const int *)nullptr, (size_t)cap, &wl))) return fail(rc);
+      if ((rc = upload<double>(c, nullptr, (size_t)cap * c->nv, &wf))) return fail(rc);
+      c->weno = WenoScratch{(unsigned int *)wc, (int *)wl, (double *)wf, cap};
+    }
+  }
   if ((rc = upload<DevCtx>(c, &c->d, 1, &c->dctx_d))) return fail(rc);
   if (cudaStreamSynchronize(c->cs) != cudaSuccess) return fail(STX_E_CUDA);
   *out = c;
@@ -395,17 +459,17 @@ int stx_euler_x(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b,
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nx) return STX_E_INVALID;
   // reads Y, rho, u, v, w, h, p, c, Ducros (ns+8) and fl (unless overwritten); writes fl
   Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.ny * c->d.g.nz * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
-  return launch_euler(c->d, c->dctx_d, S(s), 0, wa, fl, a, b, ow);
+  return launch_euler(c->d, c->dctx_d, S(s), 0, wa, fl, a, b, ow, c->weno_list[0] ? &c->weno : nullptr);
 }
 int stx_euler_y(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.ny) return STX_E_INVALID;
   Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.nx * c->d.g.nz * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
-  return launch_euler(c->d, c->dctx_d, S(s), 1, wa, fl, a, b, ow);
+  return launch_euler(c->d, c->dctx_d, S(s), 1, wa, fl, a, b, ow, c->weno_list[1] ? &c->weno : nullptr);
 }
 int stx_euler_z(stx_ctx *c, void *s, const double *wa, double *fl, int a, int b, int ow) {
   if (!c || !wa || !fl || a < 1 || b > c->d.g.nz) return STX_E_INVALID;
   Prof pf(c, S(s), STX_K_EULER, 1, (double)(b - a + 1) * c->d.g.nx * c->d.g.ny * B8(c->ns + 8 + (ow ? 1 : 2) * c->nv));
-  return launch_euler(c->d, c->dctx_d, S(s), 2, wa, fl, a, b, ow);
+  return launch_euler(c->d, c->dctx_d, S(s), 2, wa, fl, a, b, ow, c->weno_list[2] ? &c->weno : nullptr);
 }
 
 int stx_visflx(stx_ctx *c, void *s, const double *wa, double *fl, int mode) {
@@ -504,14 +568,16 @@ int stx_batch0d_integrate(stx_ctx *c, void *s, int n, const double *T0, const do
   DevCtx d = c->d;
   d.p.ros_maxsteps = max_steps;
   Prof pf(c, S(s), STX_K_CHEM, 1, (double)n * 8.0 * (2 * c->d.t.ns + 6));
-  // one warp per reactor where the mechanism fits (ns <= 32, nr <= 64): the
-  // launch lasts as long as its slowest reactor, and a warp integrates one
-  // reactor several times faster than a thread does; STX_BATCH0D_KERNEL=thread
-  // selects the thread-per-reactor kernel
+  // One warp per reactor where the mechanism fits (ns <= 32, nr <= 64) and every
+  // reactor gets a resident warp at once: a warp integrates one reactor several
+  // times faster than a thread, so a small batch (a served one) ends sooner.
+  // Larger batches run a thread per reactor (more reactors at once).
+  // STX_BATCH0D_KERNEL=thread / warp forces either kernel.
   const char *kind = std::getenv("STX_BATCH0D_KERNEL");
   if (!(kind && std::strcmp(kind, "thread") == 0)) {
+    int force = kind && std::strcmp(kind, "warp") == 0;
     int rc = launch_batch0d_warp(d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end,
-                                 nsteps, c->counter_d);
+                                 nsteps, c->counter_d, force);
     if (rc != STX_E_UNSUPPORTED) return rc;
   }
   return launch_batch0d(d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end, nsteps,
@@ -709,6 +775,124 @@ int stx_status(stx_ctx *c, void *s, uint32_t *bits, int reset) {
   STX_CUDA_TRY(cudaMemcpyAsync(&h, c->status_d, sizeof(h), cudaMemcpyDeviceToHost, S(s)));
   STX_CUDA_TRY(cudaStreamSynchronize(S(s)));
   *bits = h;
+  if (reset) STX_CUDA_TRY(cudaMemsetAsync(c->status_d, 0, sizeof(unsigned int), S(s)));
+  return STX_OK;
+}
+
+// ------------------------------------------------------------------ tuning
+int stx_get_tuning(stx_ctx *c, stx_tuning *out) {
+  if (!c || !out) return STX_E_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  for (int q = 0; q < 3; q++) {
+    out->sweep_kind[q] = c->d.p.sweep_kind[q];
+    out->weno_list[q] = c->weno_list[q];
+  }
+  out->chem_ctas_per_sm = c->d.p.chem_ctas_per_sm;
+  out->chem_ctas_max = chem_ctas_limit(c->ns);
+  return STX_OK;
+}
+
+int stx_set_tuning(stx_ctx *c, const stx_tuning *t) {
+  if (!c || !t) return STX_E_INVALID;
+  for (int q = 0; q < 3; q++)
+    if ((t->sweep_kind[q] != 0 && t->sweep_kind[q] != 1) || (t->weno_list[q] != 0 && t->weno_list[q] != 1))
+      return STX_E_INVALID;
+  if (t->chem_ctas_per_sm < 0) return STX_E_INVALID;
+  for (int q = 0; q < 3; q++) {
+    c->d.p.sweep_kind[q] = t->sweep_kind[q];
+    c->weno_list[q] = t->weno_list[q];
+  }
+  c->d.p.chem_ctas_per_sm = t->chem_ctas_per_sm;
+  STX_CUDA_TRY(cudaMemcpyAsync((void *)c->dctx_d, &c->d, sizeof(DevCtx), cudaMemcpyHostToDevice, c->cs));
+  STX_CUDA_TRY(cudaStreamSynchronize(c->cs));
+  return STX_OK;
+}
+
+int stx_autotune(stx_ctx *c, void *sv, const stx_fields *f, double dt_chem, stx_tuning *out) {
+  if (!c || !f || !f->w || !f->w_aux) return STX_E_INVALID;
+  cudaStream_t s = S(sv);
+  const DevGrid &g = c->d.g;
+  const size_t nfl = (size_t)g.npi * c->nv, nw = (size_t)g.npg * c->nv;
+  cudaMemPool_t pool = ctx_pool(c->device);
+  double *fls = nullptr, *w2 = nullptr;
+  unsigned int *st_save = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = STX_OK;
+  float sweep_ms[3] = {0.f, 0.f, 0.f}, chem_ms = 0.f;
+  if (!pool || cudaMallocFromPoolAsync((void **)&fls, nfl * sizeof(double), pool, s) != cudaSuccess ||
+      cudaMallocFromPoolAsync((void **)&st_save, sizeof(unsigned int), pool, s) != cudaSuccess)
+    return STX_E_NOMEM;
+  // the status bits the trial launches raise are not the caller's: saved here, restored at the end
+  cudaMemcpyAsync(st_save, c->status_d, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  // ---- convective sweeps: staged tiles with listed WENO faces, staged tiles
+  // with WENO in line, one face per thread (a scratch residual, overwritten)
+  const int nsw[3] = {g.nx, g.ny, g.nz};
+  for (int d = 0; d < 3 && rc == STX_OK; d++) {
+    if (d > 0 && nsw[d] == 1) continue;     // the step skips a sweep over one cell
+    struct Cand { int kind, list; };
+    const Cand cands[3] = {{0, 1}, {0, 0}, {1, 0}};
+    float best = -1.f;
+    Cand pick = cands[0];
+    for (const Cand &k : cands) {
+      if (k.list && c->weno.cap == 0) continue;
+      c->d.p.sweep_kind[d] = k.kind;
+      const WenoScratch *wsc = k.list ? &c->weno : nullptr;
+      float ms = time_launches(s, e0, e1, 3, [&] {
+        return launch_euler(c->d, c->dctx_d, s, d, f->w_aux, fls, 1, nsw[d], 1, wsc);
+      });
+      if (ms < 0.f) { rc = STX_E_CUDA; break; }
+      if (best < 0.f || ms < best) { best = ms; pick = k; }
+    }
+    c->d.p.sweep_kind[d] = pick.kind;
+    c->weno_list[d] = pick.list;
+    sweep_ms[d] = best;
+  }
+  // ---- cell chemistry (ROK4): persistent CTAs per SM, on a scratch copy of w
+  const stx_params &p = c->par;
+  if (rc == STX_OK && p.enable_chemistry == 2 && p.rosenbrock_version == 2 && dt_chem > 0.0) {
+    if (cudaMallocFromPoolAsync((void **)&w2, nw * sizeof(double), pool, s) != cudaSuccess) {
+      rc = STX_E_NOMEM;
+    } else {
+      const int lim = chem_ctas_limit(c->ns);
+      float best = -1.f;
+      int pick = 0;
+      for (int k = 1; k <= lim && rc == STX_OK; k++) {
+        c->d.p.chem_ctas_per_sm = k;
+        float ms = time_launches(s, e0, e1, 1, [&] {
+          if (cudaMemcpyAsync(w2, f->w, nw * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return (int)STX_E_CUDA;
+          return launch_rok4(c->d, s, w2, f->w_aux, nullptr, dt_chem, 0.0, dt_chem, 0, c->counter_d);
+        });
+        if (ms < 0.f) { rc = STX_E_CUDA; break; }
+        if (best < 0.f || ms < best) { best = ms; pick = k; }
+      }
+      c->d.p.chem_ctas_per_sm = pick == lim ? 0 : pick;
+      chem_ms = best;
+    }
+  }
+  cudaMemcpyAsync(c->status_d, st_save, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s);
+  if (w2) cudaFreeAsync(w2, s);
+  cudaFreeAsync(fls, s);
+  cudaFreeAsync(st_save, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess && rc == STX_OK) rc = STX_E_CUDA;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != STX_OK) return rc;
+  STX_CUDA_TRY(cudaMemcpyAsync((void *)c->dctx_d, &c->d, sizeof(DevCtx), cudaMemcpyHostToDevice, c->cs));
+  STX_CUDA_TRY(cudaStreamSynchronize(c->cs));
+  if (out) {
+    TRY(stx_get_tuning(c, out));
+    for (int d = 0; d < 3; d++) out->sweep_ms[d] = sweep_ms[d];
+    out->chem_ms = chem_ms;
+  }
+  return STX_OK;
+}
+
+int stx_status_enqueue(stx_ctx *c, void *s, uint32_t *bits, int reset) {
+  if (!c || !bits) return STX_E_INVALID;
+  STX_CUDA_TRY(cudaMemcpyAsync(bits, c->status_d, sizeof(unsigned int), cudaMemcpyDefault, S(s)));
   if (reset) STX_CUDA_TRY(cudaMemsetAsync(c->status_d, 0, sizeof(unsigned int), S(s)));
   return STX_OK;
 }

@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
     T[r] = f.T_final;
     t_ign[r] = f.t_ign;
     t_end[r] = f.time_reached;
+    __threadfence_system();   // nsteps last (see k_batch0d_w)
     nsteps[r] = f.steps;
   }
 }
@@ -317,20 +318,33 @@ __global__ void __launch_bounds__(128) k_chem_explicit(DevCtx c, double *__restr
   for (int s = 0; s < NS; s++) FI(fl, tid, s + 1) = src[s];
 }
 
-static int persistent_blocks(const void *fn, int block) {
+// persistent grid: want CTAs per SM (0 or above the occupancy limit: the limit)
+static int persistent_blocks(const void *fn, int block, int want = 0) {
   int dev = 0, nsm = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0);
   if (per < 1) per = 1;
+  if (want > 0 && want < per) per = want;
   return nsm * per;
+}
+
+int chem_ctas_limit(int ns) {
+  int per = 1;
+  switch (ns) {
+#define X(N) case N: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)k_rok4<N>, chem_block(N), 0); break;
+    STX_FOR_NS(X)
+#undef X
+    default: return 0;
+  }
+  return per < 1 ? 1 : per;
 }
 
 template <int NS>
 static int rok4_t(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
                   double t0, double t1, int simpler, unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
-  int nb = persistent_blocks((const void *)k_rok4<NS>, chem_block(NS));
+  int nb = persistent_blocks((const void *)k_rok4<NS>, chem_block(NS), c.p.chem_ctas_per_sm);
   long long need = (c.g.npi + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
   k_rok4<NS><<<nb, chem_block(NS), 0, s>>>(c, w, wa, fl_sav, dttry, t0, t1, simpler, counter);

@@ -78,6 +78,12 @@ struct DevPar {
   // diffusive fluxes and the transport properties in FP32 (RK residual still
   // accumulated in FP64; T(e) Newton, rates, K_c and the chemistry in FP64)
   int mixed;
+  // convective sweep kernel per direction: 0 staged shared-memory tiles (where
+  // they apply), 1 one face per thread; chosen by the autotuner or by
+  // STX_EULER_KERNEL=face
+  int sweep_kind[3];
+  // persistent CTAs per SM of the cell chemistry kernels (0: occupancy limit)
+  int chem_ctas_per_sm;
 };
 
 struct DevCtx {

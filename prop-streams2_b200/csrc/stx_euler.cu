@@ -634,12 +634,414 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const DevC
   }
 }
 
+// ---------------------------------------------------------------- staged tiles
+// The sweeps above give every face its own thread, which reads its six-point
+// stencil from global memory and forms every stencil pair's KEEP factors
+// itself: each cell's internal energy is formed by twelve faces and each pair's
+// factors by up to three.  The staged sweep below works on a tile of TC cells
+// along the sweep by NL lines:
+//  1. the tile and its 3-cell halos (Y_k, u, v, w, h, p, rho, Ducros) are copied
+//     into shared memory, coalesced along i;
+//  2. every staged cell forms its internal energy once;
+//  3. every stencil pair (a, a + d), d = 1..ep_order/2, forms its KEEP mass-flux
+//     factor and energy term once (the same operations as central_flux);
+//  4. every face sums its pairs from shared memory (the faces the Ducros sensor
+//     marks take the WENO flux from global memory, as in face_flux);
+//  5. every cell forms fl += (fhat_f - fhat_{f-1}) dxi/dx from the staged faces.
+// It covers ep_order <= 6 and weno_scheme <= 3 (the 3-cell halo) and ns <= 20
+// (shared memory); euler_r dispatches to the per-face sweeps otherwise.
+template <int NS, int DIR> struct ETile {
+  static constexpr int TC = DIR == 0 ? 64 : 16;        // cells per line updated by a CTA
+  static constexpr int NL = DIR == 0 ? 2 : 16;         // lines per CTA
+  static constexpr int H = 3;                          // halo cells each side
+  static constexpr int S = TC + 2 * H;                 // staged cells per line
+  static constexpr int NF = TC + 1;                    // faces per line
+  static constexpr int NP = TC + 3;                    // pair origins per line and distance
+  static constexpr int NVC = NS + 7;                   // staged fields
+  static constexpr int NT = TC * NL;                   // threads
+  // x sweep: the sweep is the contiguous direction, lines are rows (j, k);
+  // y / z sweeps: lines are consecutive i
+  __device__ static int sx(int s, int l) { return DIR == 0 ? l * S + s : s * NL + l; }
+  __device__ static int px(int a, int l) { return DIR == 0 ? l * NP + a : a * NL + l; }
+  __device__ static int fx(int f, int l) { return DIR == 0 ? l * NF + f : f * NL + l; }
+};
+
+template <int NS, typename R>
+__host__ __device__ constexpr size_t etile_smem(int dir) {
+  // cells (double) + faces (R) + pair factors (2 x 3 distances, R) + internal energy (R)
+  return dir == 0 ? (size_t)ETile<NS, 0>::NVC * ETile<NS, 0>::S * ETile<NS, 0>::NL * 8 +
+                        (size_t)(NS + 4) * ETile<NS, 0>::NF * ETile<NS, 0>::NL * sizeof(R) +
+                        (size_t)6 * ETile<NS, 0>::NP * ETile<NS, 0>::NL * sizeof(R) +
+                        (size_t)ETile<NS, 0>::S * ETile<NS, 0>::NL * sizeof(R)
+                  : (size_t)ETile<NS, 1>::NVC * ETile<NS, 1>::S * ETile<NS, 1>::NL * 8 +
+                        (size_t)(NS + 4) * ETile<NS, 1>::NF * ETile<NS, 1>::NL * sizeof(R) +
+                        (size_t)6 * ETile<NS, 1>::NP * ETile<NS, 1>::NL * sizeof(R) +
+                        (size_t)ETile<NS, 1>::S * ETile<NS, 1>::NL * sizeof(R);
+}
+
+// staged field v -> w_aux field (1-based)
+template <int NS>
+__device__ __forceinline__ int etile_field(int v) {
+  if (v < NS) return v + 1;
+  switch (v - NS) {
+    case 0: return NS + 1;    // u
+    case 1: return NS + 2;    // v
+    case 2: return NS + 3;    // w
+    case 3: return NS + 4;    // h
+    case 4: return NS + 6;    // p
+    case 5: return NS + 11;   // rho
+    default: return NS + 9;   // Ducros
+  }
+}
+
+template <int NS, int DIR, typename R>
+__global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? 4 : 2)
+    k_euler_tile(DevCtx c, const DevCtx *__restrict__ cg, const double *__restrict__ wa, double *__restrict__ fl,
+                 int nmin, int nmax, int overwrite, const double *__restrict__ fhw, long long cap) {
+  using T = ETile<NS, DIR>;
+  constexpr int TC = T::TC, NL = T::NL, S = T::S, NF = T::NF, NP = T::NP, NVC = T::NVC, NT = T::NT;
+  constexpr int NV = NS + 4;
+  constexpr int vU = NS, vV = NS + 1, vW = NS + 2, vH = NS + 3, vP = NS + 4, vR = NS + 5, vD = NS + 6;
+  const DevGrid &g = c.g;
+  extern __shared__ __align__(16) unsigned char e_smem[];
+  double *sc = (double *)e_smem;                          // [NVC][cells]
+  R *sf = (R *)(sc + NVC * S * NL);                       // [NV][faces]
+  R *sup = sf + NV * NF * NL;                             // [3][pairs] mass-flux factor
+  R *spe = sup + 3 * NP * NL;                             // [3][pairs] energy term
+  R *see = spe + 3 * NP * NL;                             // [cells] internal energy
+  const int t = threadIdx.x;
+  const int c0 = nmin + blockIdx.y * TC;                  // first cell of the tile along the sweep
+  const int nsw = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+  // line l of this CTA -> (lateral coordinates), active?
+  // x: rows r = blockIdx.x * NL + l over (j, k); y: i = blockIdx.x NL + l + 1, k = blockIdx.z + 1;
+  // z: i = blockIdx.x NL + l + 1, j = blockIdx.z + 1
+  const long long st = DIR == 0 ? 1LL : (DIR == 1 ? (long long)g.nxg : (long long)g.nxg * g.nyg);
+  auto line_base = [&](int l, bool &act) -> long long {   // gidx of the cell at sweep coordinate 0
+    if (DIR == 0) {
+      long long r = (long long)blockIdx.x * NL + l;
+      act = r < (long long)g.ny * g.nz;
+      int j = 1 + (int)(r % g.ny), k = 1 + (int)(r / g.ny);
+      return act ? gidx(g, 0, j, k) : 0;
+    } else {
+      int i = blockIdx.x * NL + l + 1;
+      act = i <= g.nx;
+      return act ? (DIR == 1 ? gidx(g, i, 0, blockIdx.z + 1) : gidx(g, i, blockIdx.z + 1, 0)) : 0;
+    }
+  };
+  // 1. stage the cells c0-3 .. c0+TC+2 of every line (zero outside the ghosted box)
+  for (int e = t; e < NVC * S * NL; e += NT) {
+    int s, l, v;
+    if (DIR == 0) { s = e % S; l = (e / S) % NL; v = e / (S * NL); }
+    else { l = e % NL; s = (e / NL) % S; v = e / (S * NL); }
+    bool act;
+    long long b = line_base(l, act);
+    int x = c0 - T::H + s;
+    double val = 0.0;
+    if (act && x >= 1 - g.ng && x <= nsw + g.ng) val = FG(wa, b + x * st, etile_field<NS>(v));
+    sc[v * S * NL + T::sx(s, l)] = val;
+  }
+  __syncthreads();
+  auto ld = [&](int v, int s, int l) -> R { return (R)sc[v * S * NL + T::sx(s, l)]; };
+  const int nkeep = c.p.nkeep;
+  int lmax = c.p.ep_order / 2;
+  if (lmax < 1) lmax = 1;
+  // 2. internal energy of every staged cell (central_flux: eei)
+  if (nkeep >= 0) {
+    for (int e = t; e < S * NL; e += NT) {
+      int s = DIR == 0 ? e % S : e / NL, l = DIR == 0 ? e / S : e % NL;
+      R rr = ld(vR, s, l), uu = ld(vU, s, l), vv = ld(vV, s, l), ww = ld(vW, s, l);
+      see[T::sx(s, l)] = ld(vH, s, l) - ld(vP, s, l) / rr - R(0.5) * (uu * uu + vv * vv + ww * ww);
+    }
+    __syncthreads();
+  }
+  // 3. pair factors for origins a = 0..TC+2 and distances d = 1..lmax
+  for (int e = t; e < lmax * NP * NL; e += NT) {
+    int d = 1 + e / (NP * NL), r = e % (NP * NL);
+    int a = DIR == 0 ? r % NP : r / NL, l = DIR == 0 ? r / NP : r % NL;
+    int b = a + d;
+    R rhoi = ld(vR, a, l), uni = ld(vU + DIR, a, l), rhoip = ld(vR, b, l), unip = ld(vU + DIR, b, l);
+    R rhom = rhoi + rhoip, drhof;
+    if (nkeep <= 0) {
+      drhof = R(1.0);
+    } else {
+      R drho = R(2.0) * (rhoip - rhoi) / rhom;
+      R tt = (R(0.5) * drho) * (R(0.5) * drho), t2 = tt;
+      R sumden = R(1.0) + tt / R(3.0);
+      for (int n = 2; n <= nkeep; n++) { int n2 = 2 * n; tt = t2 * tt; sumden = sumden + tt / (R(1.0) + n2); }
+      drhof = R(1.0) / sumden;
+    }
+    R up = (uni + unip) * rhom * drhof;
+    R pe = R(0.0);
+    if (nkeep >= 0) {
+      R eei = see[T::sx(a, l)], eeip = see[T::sx(b, l)];
+      R eem = eei + eeip, deef;
+      if (nkeep == 0) {
+        deef = R(1.0);
+      } else {
+        R dee = R(2.0) * (eeip - eei) / eem;
+        R te = (R(0.5) * dee) * (R(0.5) * dee);
+        R te2 = te;
+        R sde = R(1.0) + te, sne = R(1.0) + te / R(3.0);
+        for (int n = 2; n <= nkeep; n++) {
+          int n2 = 2 * n;
+          te = te2 * te;
+          sde = sde + te;
+          sne = sne + te / (R(1.0) + n2);
+        }
+        deef = sne / sde;
+      }
+      pe = up * eem * deef;
+    }
+    sup[(d - 1) * NP * NL + T::px(a, l)] = up;
+    spe[(d - 1) * NP * NL + T::px(a, l)] = pe;
+  }
+  __syncthreads();
+  // 4. faces c0-1 .. c0+TC-1 (staged position of face f's left cell: f - c0 + 3)
+  const int ws = c.p.weno_scheme;
+  for (int e = t; e < NF * NL; e += NT) {
+    int fr = DIR == 0 ? e % NF : e / NL, l = DIR == 0 ? e / NF : e % NL;
+    int f = c0 - 1 + fr;
+    bool act;
+    long long b = line_base(l, act);
+    if (!act || f < nmin - 1 || f > nmax) continue;
+    const int q = fr + 2;
+    R *fo = sf + T::fx(fr, l);                            // this face's fluxes, stride NF * NL
+    bool shk = false;
+    for (int s = -ws + 1; s <= ws; s++) shk |= (sc[vD * S * NL + T::sx(q + s, l)] > c.p.sensor_threshold);
+    if (!shk) {
+      bool fz = (f == 0 && c.p.fzf[2 * DIR] == 1) || (f == nsw && c.p.fzf[2 * DIR + 1] == 1);
+#pragma unroll 1
+      for (int lsp = 0; lsp < NS; lsp++) {
+        R ft1 = R(0.0);
+#pragma unroll
+        for (int ll = 1; ll <= T::H; ll++) {
+          if (ll <= lmax) {
+            R uvs1 = R(0.0);
+#pragma unroll
+            for (int m = 0; m < ll; m++)
+              uvs1 = uvs1 + sup[(ll - 1) * NP * NL + T::px(q - m, l)] * (ld(lsp, q - m, l) + ld(lsp, q - m + ll, l));
+            ft1 = ft1 + R(c.p.cd1[ll][lmax]) * uvs1;
+          }
+        }
+        fo[lsp * NF * NL] = fz ? R(0.0) : R(0.25) * ft1;
+      }
+      R ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
+#pragma unroll
+      for (int ll = 1; ll <= T::H; ll++) {
+        if (ll > lmax) break;
+        R uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs6 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0;
+#pragma unroll
+        for (int m = 0; m < ll; m++) {
+          const int a = q - m, bb = q - m + ll;
+          R uui = ld(vU, a, l), vvi = ld(vV, a, l), wwi = ld(vW, a, l), ppi = ld(vP, a, l);
+          R uuip = ld(vU, bb, l), vvip = ld(vV, bb, l), wwip = ld(vW, bb, l), ppip = ld(vP, bb, l);
+          R uni = DIR == 0 ? uui : (DIR == 1 ? vvi : wwi);
+          R unip = DIR == 0 ? uuip : (DIR == 1 ? vvip : wwip);
+          R uv_part = sup[(ll - 1) * NP * NL + T::px(a, l)];
+          uvs2 = uvs2 + uv_part * (uui + uuip);
+          uvs3 = uvs3 + uv_part * (vvi + vvip);
+          uvs4 = uvs4 + uv_part * (wwi + wwip);
+          if (nkeep >= 0) {
+            uvs5_i = uvs5_i + spe[(ll - 1) * NP * NL + T::px(a, l)];
+            uvs5_k = uvs5_k + uv_part * (uui * uuip + vvi * vvip + wwi * wwip);
+            uvs5_p = uvs5_p + R(4.0) * (uni * ppip + unip * ppi);
+          } else {
+            uvs5 = uvs5 + uv_part * (ld(vH, a, l) + ld(vH, bb, l));
+          }
+          uvs6 = uvs6 + R(2.0) * (ppi + ppip);
+        }
+        R cl = R(c.p.cd1[ll][lmax]);
+        ft2 = ft2 + cl * uvs2;
+        ft3 = ft3 + cl * uvs3;
+        ft4 = ft4 + cl * uvs4;
+        ft5 = ft5 + cl * (nkeep >= 0 ? (uvs5_i + uvs5_k + uvs5_p) : uvs5);
+        ft6 = ft6 + cl * uvs6;
+      }
+      R fm0 = R(0.25) * ft2, fm1 = R(0.25) * ft3, fm2 = R(0.25) * ft4, fh5 = R(0.25) * ft5;
+      if (fz) { fm0 = fm1 = fm2 = fh5 = R(0.0); }
+      if (DIR == 0) fm0 = fm0 + R(0.5) * ft6;
+      if (DIR == 1) fm1 = fm1 + R(0.5) * ft6;
+      if (DIR == 2) fm2 = fm2 + R(0.5) * ft6;
+      fo[NS * NF * NL] = fm0;
+      fo[(NS + 1) * NF * NL] = fm1;
+      fo[(NS + 2) * NF * NL] = fm2;
+      fo[(NS + 3) * NF * NL] = fh5;
+    } else if (fhw) {          // computed by k_weno_list
+      long long id;
+      if (DIR == 0) id = ((long long)blockIdx.x * NL + l) * (nmax - nmin + 2) + (f - nmin + 1);
+      else id = ((long long)(f - nmin + 1) * (DIR == 1 ? g.nz : g.ny) + blockIdx.z) * g.nx + (blockIdx.x * NL + l);
+#pragma unroll
+      for (int m = 0; m < NV; m++) fo[m * NF * NL] = (R)fhw[m * cap + id];
+    } else {
+      double fw[NV];
+      long long p = b + (long long)f * st;
+      if (c.p.flux_splitting == 1) weno_rusanov_flux<NS, DIR>(*cg, wa, p, st, fw);
+      else weno_char_flux<NS, DIR>(*cg, wa, p, st, fw);
+#pragma unroll
+      for (int m = 0; m < NV; m++) fo[m * NF * NL] = (R)fw[m];
+    }
+  }
+  __syncthreads();
+  // 5. divergence into fl for the cells c0 .. c0+TC-1
+  {
+    int sr = DIR == 0 ? t % TC : t / NL, l = DIR == 0 ? t / TC : t % NL;
+    int i = c0 + sr;
+    bool act;
+    line_base(l, act);
+    if (act && i <= nmax) {
+      long long qf;
+      if (DIR == 0) {
+        long long r = (long long)blockIdx.x * NL + l;
+        qf = fidx(g, i, 1 + (int)(r % g.ny), 1 + (int)(r / g.ny));
+      } else if (DIR == 1) {
+        qf = fidx(g, blockIdx.x * NL + l + 1, i, blockIdx.z + 1);
+      } else {
+        qf = fidx(g, blockIdx.x * NL + l + 1, blockIdx.z + 1, i);
+      }
+      const double *met = DIR == 0 ? g.dcsidx : (DIR == 1 ? g.detady : g.dzitdz);
+      double mt = ldg(met + i - 1);
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        double d = (double)((sf[m * NF * NL + T::fx(sr + 1, l)] - sf[m * NF * NL + T::fx(sr, l)]) * (R)mt);
+        FI(fl, qf, m + 1) = overwrite ? d : FI(fl, qf, m + 1) + d;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- listed WENO faces
+// The Ducros sensor marks a minority of the faces of a turbulent field, spread
+// over the grid; computed in line, every warp holding one marked face runs the
+// characteristic WENO flux with most of its lanes idle.  Instead, k_weno_mark
+// lists the marked faces (warp-aggregated appends), k_weno_list computes their
+// fluxes with every lane busy into a face-indexed buffer, and the staged sweep
+// reads them there.  Each face's flux is the same function of the same inputs,
+// so the result does not depend on the list's order.
+//
+// Face ids of a sweep over cells nmin..nmax (faces nmin-1..nmax, fr = f - nmin + 1,
+// nf = nmax - nmin + 2): x: row (j, k) * nf + fr; y: (fr * nz + k - 1) * nx + i - 1;
+// z: (fr * ny + j - 1) * nx + i - 1 (i fastest: coalesced along the grid).
+template <int DIR>
+__device__ __forceinline__ void weno_face(const DevGrid &g, long long id, int nmin, int nmax, long long &p, int &f) {
+  if (DIR == 0) {
+    long long nf = nmax - nmin + 2, r = id / nf;
+    f = nmin - 1 + (int)(id - r * nf);
+    p = gidx(g, f, 1 + (int)(r % g.ny), 1 + (int)(r / g.ny));
+  } else {
+    int i = 1 + (int)(id % g.nx);
+    long long t = id / g.nx;
+    int no = DIR == 1 ? g.nz : g.ny;
+    int o = 1 + (int)(t % no);
+    f = nmin - 1 + (int)(t / no);
+    p = DIR == 1 ? gidx(g, i, f, o) : gidx(g, i, o, f);
+  }
+}
+
+template <int NS, int DIR>
+__global__ void __launch_bounds__(256) k_weno_mark(DevCtx c, const double *__restrict__ wa, int nmin, int nmax,
+                                                   long long total, unsigned int *count, int *list) {
+  const DevGrid &g = c.g;
+  const int J_DUC = NS + 9, ws = c.p.weno_scheme;
+  const long long st = DIR == 0 ? 1LL : (DIR == 1 ? (long long)g.nxg : (long long)g.nxg * g.nyg);
+  const int lane = threadIdx.x & 31;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < total; base += (long long)gridDim.x * blockDim.x) {
+    long long id = base + threadIdx.x;
+    bool shk = false;
+    if (id < total) {
+      long long p;
+      int f;
+      weno_face<DIR>(g, id, nmin, nmax, p, f);
+      for (int q = -ws + 1; q <= ws; q++) shk |= (FG(wa, p + q * st, J_DUC) > c.p.sensor_threshold);
+    }
+    unsigned m = __ballot_sync(0xffffffffu, shk);
+    if (m) {
+      unsigned b0 = 0;
+      if (lane == 0) b0 = atomicAdd(count, (unsigned)__popc(m));
+      b0 = __shfl_sync(0xffffffffu, b0, 0);
+      if (shk) list[b0 + __popc(m & ((1u << lane) - 1u))] = (int)id;
+    }
+  }
+}
+
+template <int NS, int DIR>
+__global__ void __launch_bounds__(128, 4) k_weno_list(DevCtx c, const DevCtx *__restrict__ cg,
+                                                      const double *__restrict__ wa, int nmin, int nmax,
+                                                      const unsigned int *__restrict__ count,
+                                                      const int *__restrict__ list, double *__restrict__ fh,
+                                                      long long cap) {
+  const DevGrid &g = c.g;
+  const long long st = DIR == 0 ? 1LL : (DIR == 1 ? (long long)g.nxg : (long long)g.nxg * g.nyg);
+  const long long n = *count;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    long long id = list[q], p;
+    int f;
+    weno_face<DIR>(g, id, nmin, nmax, p, f);
+    double fw[NS + 4];
+    if (c.p.flux_splitting == 1) weno_rusanov_flux<NS, DIR>(*cg, wa, p, st, fw);
+    else weno_char_flux<NS, DIR>(*cg, wa, p, st, fw);
+#pragma unroll
+    for (int m = 0; m < NS + 4; m++) fh[m * cap + id] = fw[m];
+  }
+}
+
+long long weno_scratch_faces(const DevGrid &g) {
+  long long a = (long long)(g.nx + 1) * g.ny * g.nz, b = (long long)g.nx * (g.ny + 1) * g.nz,
+            d = (long long)g.nx * g.ny * (g.nz + 1);
+  long long m = a > b ? a : b;
+  return m > d ? m : d;
+}
+
+template <int NS, int DIR, typename R>
+static int euler_tile_launch(const DevCtx &c, const DevCtx *cg, cudaStream_t s, const double *wa, double *fl,
+                             int nmin, int nmax, int ow, const WenoScratch *wsc) {
+  using T = ETile<NS, DIR>;
+  const DevGrid &g = c.g;
+  // listed WENO faces where the scratch holds the sweep's faces
+  const long long lines = DIR == 0 ? (long long)g.ny * g.nz : (long long)g.nx * (DIR == 1 ? g.nz : g.ny);
+  const long long total = (long long)(nmax - nmin + 2) * lines;
+  const double *fhw = nullptr;
+  long long cap = 0;
+  if (wsc && wsc->cap >= total && total < 0x7fffffffLL) {
+    int dev = 0, nsm = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    STX_CUDA_TRY(cudaMemsetAsync(wsc->count, 0, sizeof(unsigned int), s));
+    long long nb = (total + 255) / 256;
+    if (nb > (long long)nsm * 16) nb = (long long)nsm * 16;
+    k_weno_mark<NS, DIR><<<(unsigned)nb, 256, 0, s>>>(c, wa, nmin, nmax, total, wsc->count, wsc->list);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)k_weno_list<NS, DIR>, 128, 0);
+    k_weno_list<NS, DIR><<<nsm * (per < 1 ? 1 : per), 128, 0, s>>>(c, cg, wa, nmin, nmax, wsc->count, wsc->list,
+                                                                    wsc->fh, wsc->cap);
+    STX_CUDA_TRY(cudaGetLastError());
+    fhw = wsc->fh;
+    cap = wsc->cap;
+  }
+  constexpr size_t smem = etile_smem<NS, R>(DIR);   // opted in by launch_euler_setup
+  long long tiles = (nmax - nmin + 1 + T::TC - 1) / T::TC;
+  long long lgrp = DIR == 0 ? ((long long)g.ny * g.nz + T::NL - 1) / T::NL : (g.nx + T::NL - 1) / T::NL;
+  int other = DIR == 0 ? 1 : (DIR == 1 ? g.nz : g.ny);
+  if (lgrp > 0x7fffffffLL || tiles > 65535 || other > 65535) return STX_E_INVALID;
+  // sweep tiles in gridDim.y: the tiles that share halos run close together
+  dim3 grid((unsigned)lgrp, (unsigned)tiles, (unsigned)other);
+  k_euler_tile<NS, DIR, R><<<grid, T::NT, smem, s>>>(c, cg, wa, fl, nmin, nmax, ow, fhw, cap);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
 template <int NS, typename R>
 static int euler_r(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
-                   int nmax, int ow) {
+                   int nmax, int ow, const WenoScratch *wsc) {
   const DevGrid &g = c.g;
   if (nmax - nmin < 0) return STX_OK;
   if (2 * c.p.weno_scheme > WMAX) return STX_E_UNSUPPORTED;
+  // staged tiles where they apply and the context selects them (the default)
+  if (NS <= 14 && c.p.ep_order / 2 <= 3 && c.p.weno_scheme <= 3 && g.ng >= 3 && c.p.sweep_kind[dir] == 0) {
+    if constexpr (NS <= 14) {
+      if (dir == 0) return euler_tile_launch<NS, 0, R>(c, cg, s, wa, fl, nmin, nmax, ow, wsc);
+      if (dir == 1) return euler_tile_launch<NS, 1, R>(c, cg, s, wa, fl, nmin, nmax, ow, wsc);
+      return euler_tile_launch<NS, 2, R>(c, cg, s, wa, fl, nmin, nmax, ow, wsc);
+    }
+  }
   if (dir == 0) {
     long long nface = (long long)(nmax - nmin + 2) * g.ny * g.nz;
     constexpr int XB = xsweep_block(NS);
@@ -660,15 +1062,45 @@ static int euler_r(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, c
 // the plain form computes the central faces in FP64, the mixed form in FP32
 template <int NS>
 static int euler_t(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
-                   int nmax, int ow) {
-  return c.p.mixed ? euler_r<NS, float>(c, cg, s, dir, wa, fl, nmin, nmax, ow)
-                   : euler_r<NS, double>(c, cg, s, dir, wa, fl, nmin, nmax, ow);
+                   int nmax, int ow, const WenoScratch *wsc) {
+  return c.p.mixed ? euler_r<NS, float>(c, cg, s, dir, wa, fl, nmin, nmax, ow, wsc)
+                   : euler_r<NS, double>(c, cg, s, dir, wa, fl, nmin, nmax, ow, wsc);
+}
+
+// the staged sweeps' shared memory exceeds the 48 KB default: opt in once per
+// instantiation, outside any stream capture (at context creation)
+template <int NS>
+static int euler_setup_t() {
+  if constexpr (NS <= 14) {
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, double>(0)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, double>(1)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, double>(2)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, float>(0)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, float>(1)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, float>(2)));
+  }
+  return STX_OK;
+}
+
+int launch_euler_setup(int ns) {
+  switch (ns) {
+#define X(N) case N: return euler_setup_t<N>();
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
 }
 
 int launch_euler(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
-                 int nmax, int ow) {
+                 int nmax, int ow, const WenoScratch *wsc) {
   switch (c.t.ns) {
-#define X(N) case N: return euler_t<N>(c, cg, s, dir, wa, fl, nmin, nmax, ow);
+#define X(N) case N: return euler_t<N>(c, cg, s, dir, wa, fl, nmin, nmax, ow, wsc);
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;

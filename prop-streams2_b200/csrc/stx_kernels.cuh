@@ -14,12 +14,28 @@ int launch_update_field(const DevCtx &c, cudaStream_t s, double *w, const double
                         const int32_t *mask, double gamdt, int fused);
 int launch_compute_dt(const DevCtx &c, cudaStream_t s, const double *wa, const int32_t *mask, unsigned long long *out9);
 
-// cg: a device-resident copy of c, for the out-of-line WENO face fluxes
+// Scratch of the listed WENO faces (stx_euler.cu): a counter, the ids of the
+// faces the Ducros sensor marks, and their fluxes by face id (nv x cap).
+struct WenoScratch {
+  unsigned int *count;
+  int *list;
+  double *fh;
+  long long cap;      // faces the buffers hold (0: no scratch)
+};
+// faces of the largest sweep of a grid (the listed-WENO scratch size)
+long long weno_scratch_faces(const DevGrid &g);
+
+// once per context, before any capture: kernel attributes of the staged sweeps
+int launch_euler_setup(int ns);
+// cg: a device-resident copy of c, for the out-of-line WENO face fluxes;
+// ws: the listed-WENO scratch (null or cap 0: WENO faces computed in line)
 int launch_euler(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,
-                 int nmax, int overwrite);
+                 int nmax, int overwrite, const WenoScratch *ws);
 int launch_visflx(const DevCtx &c, cudaStream_t s, int dir, const double *wa, double *fl);
 int launch_visflx_reduced(const DevCtx &c, cudaStream_t s, const double *wa, double *fl);
 
+// occupancy limit (CTAs per SM) of the ROK4 cell kernel for ns species
+int chem_ctas_limit(int ns);
 int launch_rok4(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
                 double t0, double t1, int simpler, unsigned int *counter);
 int launch_rosenbrock(const DevCtx &c, cudaStream_t s, double *w, double *wa, double dttry, double t0, double t1,
@@ -28,7 +44,8 @@ int launch_chem_explicit(const DevCtx &c, cudaStream_t s, double *w, double *wa,
 int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
                    double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
                    double *t_end, int *nsteps, unsigned int *counter);
-// one warp per reactor (ns <= 32, nr <= 64; STX_E_UNSUPPORTED otherwise)
+// one warp per reactor (ns <= 32, nr <= 64, and unless force, no more reactors
+// than resident warps; STX_E_UNSUPPORTED otherwise)
 int launch_batch0d_warp(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
                         double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
-                        double *t_end, int *nsteps, unsigned int *counter);
+                        double *t_end, int *nsteps, unsigned int *counter, int force);

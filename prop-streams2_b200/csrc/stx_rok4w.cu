@@ -296,26 +296,34 @@ __global__ void __launch_bounds__(128) k_batch0d_w(DevCtx c, int n, const double
       T[r] = f.T_final;
       t_ign[r] = f.t_ign;
       t_end[r] = f.time_reached;
-      nsteps[r] = f.steps;
     }
+    // nsteps last, after every lane's outputs are visible system-wide: a caller
+    // whose outputs are mapped host memory polls it to collect finished reactors
+    __threadfence_system();
+    __syncwarp();
+    if (lane == 0) nsteps[r] = f.steps;
   }
 }
 
 template <int NS>
 static int batch0d_w_t(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
                        double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
-                       double *t_end, int *nsteps, unsigned int *counter) {
+                       double *t_end, int *nsteps, unsigned int *counter, int force) {
   if constexpr (NS > 32) {
     return STX_E_UNSUPPORTED;
   } else {
   if (c.t.nr > WNRMAX) return STX_E_UNSUPPORTED;
-  STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
   int dev = 0, nsm = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)k_batch0d_w<NS>, 128, 0);
   long long nb = (long long)nsm * (per < 1 ? 1 : per);
   long long need = ((long long)n + 3) / 4;      // four reactors (warps) per CTA
+  // More reactors than resident warps: a thread per reactor finishes the batch
+  // sooner (all of them run at once); the warp kernel only where every reactor
+  // gets its own warp from the start, unless forced.
+  if (!force && need > nb) return STX_E_UNSUPPORTED;
+  STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
   if (nb > need) nb = need;
   k_batch0d_w<NS><<<(int)nb, 128, 0, s>>>(c, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps,
                                           counter);
@@ -326,9 +334,9 @@ static int batch0d_w_t(const DevCtx &c, cudaStream_t s, int n, const double *T0,
 
 int launch_batch0d_warp(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
                         double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
-                        double *t_end, int *nsteps, unsigned int *counter) {
+                        double *t_end, int *nsteps, unsigned int *counter, int force) {
   switch (c.t.ns) {
-#define X(N) case N: return batch0d_w_t<N>(c, s, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps, counter);
+#define X(N) case N: return batch0d_w_t<N>(c, s, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps, counter, force);
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;

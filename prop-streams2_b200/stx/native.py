@@ -72,6 +72,11 @@ class StxKprof(C.Structure):
     _fields_ = [("launches", C.c_int64), ("timed", C.c_int64), ("ms", C.c_double), ("bytes", C.c_double)]
 
 
+class StxTuning(C.Structure):
+    _fields_ = [("sweep_kind", C.c_int32 * 3), ("weno_list", C.c_int32 * 3), ("chem_ctas_per_sm", C.c_int32),
+                ("chem_ctas_max", C.c_int32), ("sweep_ms", C.c_float * 3), ("chem_ms", C.c_float)]
+
+
 _VP = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -111,6 +116,10 @@ STX_SIGNATURES = [
     ("stx_rk_sync", _I, [_VP, _VP, C.POINTER(StxFields), _D, _I]),
     ("stx_advance_solution", _I, [_VP, _VP, C.POINTER(StxFields), _D, _D]),
     ("stx_status", _I, [_VP, _VP, C.POINTER(C.c_uint32), _I]),
+    ("stx_status_enqueue", _I, [_VP, _VP, _VP, _I]),
+    ("stx_get_tuning", _I, [_VP, C.POINTER(StxTuning)]),
+    ("stx_set_tuning", _I, [_VP, C.POINTER(StxTuning)]),
+    ("stx_autotune", _I, [_VP, _VP, C.POINTER(StxFields), _D, C.POINTER(StxTuning)]),
     ("stx_profile_enable", _I, [_VP, _I]),
     ("stx_profile_read", _I, [_VP, C.POINTER(StxKprof)]),
 ]

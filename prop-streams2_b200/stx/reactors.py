@@ -103,6 +103,31 @@ class BatchReactors:
             torch.cuda.current_stream(self.device).synchronize()
         return out
 
+    def launch(self, T0: torch.Tensor, p0: torch.Tensor, Y0: torch.Tensor, out: dict, t_max: float,
+               dttry: float = 1e-8, ign_factor: float = 1.05, end_factor: float = 2.0, max_steps: int = 100000):
+        """Launch n reactors on the current stream with caller-owned buffers and
+        return at once.  Every tensor is either on the device or in pinned host
+        memory (read and written by the kernel in place, no copies): T0, p0 (n,),
+        Y0 (ns, n) float64 contiguous; out holds Y, T, t_ign, t_end (float64) and
+        nsteps (int32) of the same shapes.  The kernel writes a reactor's nsteps
+        after its other outputs, behind a system-scope fence, so with nsteps in
+        pinned host memory preset to -1 the caller can collect each reactor as
+        soon as its nsteps turns non-negative, before the launch ends."""
+        n = T0.numel()
+        ts = [T0, p0, Y0] + [out[k] for k in ("Y", "T", "t_ign", "t_end", "nsteps")]
+        for t in ts:
+            if not t.is_contiguous() or not (t.is_cuda or t.is_pinned()):
+                raise ValueError("launch needs contiguous device or pinned host tensors")
+        if p0.numel() != n or tuple(Y0.shape) != (self.ns, n) or tuple(out["Y"].shape) != (self.ns, n):
+            raise ValueError(f"expected T0, p0 of shape ({n},) and Y0, Y of shape ({self.ns}, {n})")
+        if any(out[k].numel() != n for k in ("T", "t_ign", "t_end", "nsteps")) or out["nsteps"].dtype != torch.int32:
+            raise ValueError("out: T, t_ign, t_end float64 and nsteps int32 of n entries")
+        vp = lambda t: C.c_void_p(t.data_ptr())
+        check(self.lib.stx_batch0d_integrate(self.ctx, self.stream(), n, vp(T0), vp(p0), vp(Y0), t_max, dttry,
+                                             ign_factor, end_factor, max_steps, vp(out["Y"]), vp(out["T"]),
+                                             vp(out["t_ign"]), vp(out["t_end"]), vp(out["nsteps"])),
+              "stx_batch0d_integrate")
+
     def status(self, reset: bool = True) -> int:
         bits = C.c_uint32()
         check(self.lib.stx_status(self.ctx, self.stream(), C.byref(bits), int(reset)), "stx_status")

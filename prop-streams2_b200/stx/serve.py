@@ -9,13 +9,19 @@ sizes arrive over time and share the device:
   work counter and stream) is free, every reactor request that has arrived is
   launched in one persistent stx_batch0d_integrate launch on it, so requests
   that arrive while batches run start in the next free lane, concurrently
-  with the running ones;
+  with the running ones.  A lane's inputs and outputs live in pinned host
+  memory that the kernel reads and writes in place; the kernel publishes each
+  reactor's step count last, behind a system-scope fence, so the loop
+  completes every reactor as soon as it is done instead of when its batch
+  ends;
 * grid requests (1-D flames, 2-D shock tubes; fixed dt, so no host
   synchronisation inside a step) each get their own solver context, fields in
   HBM and CUDA stream, and are admitted in arrival order while the memory
   budget and the slot count allow; the loop enqueues a few steps at a time on
-  every active request's stream, so their kernels overlap on the device, and
-  frees the slot as soon as a request has done its steps.
+  every active request's stream, so their kernels overlap on the device, then
+  enqueues the result's copies into pinned host buffers and frees the slot
+  when they have landed.  Nothing in the loop waits on the device: it polls
+  events (and, for reactors, the step counts in host memory).
 
 A request's result does not depend on what else runs: every kernel's result
 per cell or reactor is independent of the launch's other work (the
@@ -25,6 +31,7 @@ Latency is completion minus arrival, measured on the host clock.
 """
 from __future__ import annotations
 
+import ctypes as C
 import dataclasses
 import time
 from typing import Dict, List, Optional
@@ -34,6 +41,7 @@ import torch
 
 from . import configs
 from . import mech as M
+from .native import check
 from .reactors import BatchReactors
 from .solver import Solver
 
@@ -59,6 +67,66 @@ class _GridJob:
         self.req, self.sol, self.stream, self.nbytes = req, solver, stream, nbytes
         self.steps_done = 0
         self.event: Optional[torch.cuda.Event] = None
+        self.host: Optional[dict] = None      # pinned result buffers while draining
+
+
+class _ReactorLane:
+    """A reactor lane: a context (its own work counter), a stream, and pinned
+    host buffers of `cap` reactors that the kernel reads and writes in place."""
+
+    def __init__(self, br: BatchReactors, stream: torch.cuda.Stream, cap: int):
+        self.br, self.stream, self.cap = br, stream, cap
+        ns = br.ns
+        f64 = dict(dtype=torch.float64, pin_memory=True)
+        self.T0, self.p0 = torch.empty(cap, **f64), torch.empty(cap, **f64)
+        self.Y0, self.Y = torch.empty(ns * cap, **f64), torch.empty(ns * cap, **f64)
+        self.T, self.t_ign, self.t_end = (torch.empty(cap, **f64) for _ in range(3))
+        self.nsteps = torch.empty(cap, dtype=torch.int32, pin_memory=True)
+        self.reqs: Optional[List[Request]] = None
+        self.event: Optional[torch.cuda.Event] = None
+        self.collected: Optional[np.ndarray] = None
+
+    @property
+    def busy(self) -> bool:
+        return self.reqs is not None
+
+    def launch(self, reqs: List[Request], t_max: float, max_steps: int):
+        """Launch the requests' reactors, coldest first (the longest integrations
+        start first)."""
+        n, ns = len(reqs), self.br.ns
+        T0 = np.array([r.params["T0"] for r in reqs])
+        order = np.argsort(T0, kind="stable")
+        reqs = [reqs[i] for i in order]
+        self.T0.numpy()[:n] = T0[order]
+        self.p0.numpy()[:n] = [r.params["p0"] for r in reqs]
+        Y0 = self.Y0[:ns * n].view(ns, n)
+        Y0.numpy()[:] = np.stack([r.params["Y0"] for r in reqs], axis=1)
+        self.nsteps.numpy()[:n] = -1
+        out = {"Y": self.Y[:ns * n].view(ns, n), "T": self.T[:n], "t_ign": self.t_ign[:n], "t_end": self.t_end[:n],
+               "nsteps": self.nsteps[:n]}
+        with torch.cuda.stream(self.stream):
+            self.br.launch(self.T0[:n], self.p0[:n], Y0, out, t_max, 1e-8, 1.05, 2.0, max_steps)
+            self.event = torch.cuda.Event()
+            self.event.record(self.stream)
+        self.reqs = reqs
+        self.collected = np.zeros(n, dtype=bool)
+
+    def poll(self, now: float) -> int:
+        """Complete the reactors whose results have arrived; free the lane when the
+        launch has ended.  Returns the number completed."""
+        n, ns = len(self.reqs), self.br.ns
+        fresh = np.nonzero((self.nsteps.numpy()[:n] >= 0) & ~self.collected)[0]
+        if fresh.size:
+            Y = self.Y.numpy()[:ns * n].reshape(ns, n)
+            T, ti, te, st = (a.numpy() for a in (self.T, self.t_ign, self.t_end, self.nsteps))
+            for i in fresh:
+                self.reqs[i].result = {"Y": Y[:, i].copy(), "T": float(T[i]), "t_ign": float(ti[i]),
+                                       "t_end": float(te[i]), "nsteps": int(st[i])}
+                self.reqs[i].done = now
+            self.collected[fresh] = True
+        if self.collected.all() and self.event.query():
+            self.reqs = None
+        return int(fresh.size)
 
 
 class Server:
@@ -66,34 +134,48 @@ class Server:
 
     mem_budget: bytes of HBM the grid solves may hold at once; max_grid: most
     grid solves in flight; chunk: steps enqueued per grid solve per pass;
-    reactor_batch: most reactors per batched launch."""
+    reactor_batch: most reactors per batched launch (the default, 1024, stays
+    within the reactors the warp-per-reactor kernel runs at once on a B200, so
+    every served batch, like a request served alone, takes that kernel)."""
 
     def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 32, chunk: int = 5,
-                 reactor_batch: int = 16384, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 4):
+                 reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 4):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         torch.cuda.set_device(self.device)
         rtab = M.build_tables(configs.mechanism("h2air_9sp"), 101325.0, 200.0, 5500.0, 1.0)
-        self.lanes = [BatchReactors("h2air_9sp", device=str(self.device), tables=rtab) for _ in range(reactor_lanes)]
-        self.lane_streams = [torch.cuda.Stream(self.device) for _ in range(reactor_lanes)]
-        self.reactors = self.lanes[0]
+        self.lanes = [_ReactorLane(BatchReactors("h2air_9sp", device=str(self.device), tables=rtab),
+                                   torch.cuda.Stream(self.device), reactor_batch) for _ in range(reactor_lanes)]
+        self.reactors = self.lanes[0].br
         self.tables = {
             "flame1d": M.build_tables(configs.mechanism("h2air_9sp"), 101325.0, 200.0, 5500.0, 1.0),
             "tube2d": M.build_tables(configs.mechanism("shock_tube_9sp"), 7173.0, 200.0, 20000.0, 1.0),
         }
         self.mem_budget, self.max_grid, self.chunk = mem_budget, max_grid, chunk
         self.reactor_batch, self.t_max, self.max_steps = reactor_batch, t_max, max_steps
+        self._cases: Dict[tuple, object] = {}
 
     # ------------------------------------------------------------------ grid solves
     def _case(self, req: Request):
-        p = req.params
-        if req.kind == "flame1d":
-            return configs.flame_case(p["nx"], phi=p["phi"], Tu=p["Tu"], tables=self.tables["flame1d"],
-                                      mech_name="h2air_9sp")
-        if req.kind == "tube2d":
-            return configs.tube_case(p["nx"], p["ny"], tables=self.tables["tube2d"])
-        raise ValueError(req.kind)
+        """The request's case (host initial fields and parameters).  Cases are
+        read-only once built, so requests with the same parameters share one
+        (a small cache: the shock tubes of the mix are all alike)."""
+        key = (req.kind, tuple(sorted(req.params.items())))
+        case = self._cases.pop(key, None)
+        if case is None:
+            p = req.params
+            if req.kind == "flame1d":
+                case = configs.flame_case(p["nx"], phi=p["phi"], Tu=p["Tu"], tables=self.tables["flame1d"],
+                                          mech_name="h2air_9sp")
+            elif req.kind == "tube2d":
+                case = configs.tube_case(p["nx"], p["ny"], tables=self.tables["tube2d"])
+            else:
+                raise ValueError(req.kind)
+        self._cases[key] = case                      # most recently used last
+        while len(self._cases) > 8:
+            self._cases.pop(next(iter(self._cases)))
+        return case
 
     @staticmethod
     def grid_bytes(case) -> int:
@@ -105,7 +187,8 @@ class Server:
         case = self._case(req)
         stream = torch.cuda.Stream(self.device)
         with torch.cuda.stream(stream):
-            sol = Solver(case, device=str(self.device))
+            # a fresh case's w_aux holds only the temperature guess
+            sol = Solver(case, device=str(self.device), aux_slots=(case.J("T"),))
             sol.prepare()
         req.admitted = now
         return _GridJob(req, sol, stream, self.grid_bytes(case))
@@ -119,38 +202,28 @@ class Server:
             job.event.record(job.stream)
         job.steps_done += n
 
-    def _finish_grid(self, job: _GridJob, now: float):
+    def _drain_grid(self, job: _GridJob):
+        """Enqueue the result's copies into pinned host buffers (and the status
+        word) on the job's stream; the loop completes the job when they land."""
+        sol = job.sol
+        h = {"w": torch.empty(sol.w.shape, dtype=torch.float64, pin_memory=True),
+             "T": torch.empty(sol.w_aux.shape[1:], dtype=torch.float64, pin_memory=True),
+             "status": torch.zeros(1, dtype=torch.int32, pin_memory=True)}
         with torch.cuda.stream(job.stream):
-            w = job.sol.w.cpu().numpy()
-            T = job.sol.w_aux[job.sol.case.J("T")].cpu().numpy()
-        job.req.result = {"w": w, "T": job.sol.case.interior(T), "status": job.sol.status()}
+            h["w"].copy_(sol.w, non_blocking=True)
+            h["T"].copy_(sol.w_aux[sol.case.J("T")], non_blocking=True)
+            check(sol.lib.stx_status_enqueue(sol.ctx, sol.stream, C.c_void_p(h["status"].data_ptr()), 1),
+                  "stx_status_enqueue")
+            job.event = torch.cuda.Event()
+            job.event.record(job.stream)
+        job.host = h
+
+    def _finish_grid(self, job: _GridJob, now: float):
+        h = job.host
+        job.req.result = {"w": h["w"].numpy().copy(), "T": job.sol.case.interior(h["T"].numpy()).copy(),
+                          "status": int(h["status"].numpy()[0]) & 0xffffffff}
         job.req.done = now
         job.sol.close()
-
-    # ------------------------------------------------------------------ reactors
-    def _launch_reactors(self, lane: int, reqs: List[Request], now: float):
-        T0 = np.array([r.params["T0"] for r in reqs])
-        p0 = np.array([r.params["p0"] for r in reqs])
-        Y0 = np.stack([r.params["Y0"] for r in reqs], axis=1)
-        st = self.lane_streams[lane]
-        with torch.cuda.stream(st):
-            out = self.lanes[lane].integrate(T0, p0, Y0, self.t_max, 1e-8, 1.05, 2.0, self.max_steps, sync=False,
-                                             order="coldest_first")
-            ev = torch.cuda.Event()
-            ev.record(st)
-        for r in reqs:
-            r.admitted = now
-        return reqs, out, ev, st
-
-    def _finish_reactors(self, batch, now: float):
-        reqs, out, ev, st = batch
-        ev.synchronize()
-        with torch.cuda.stream(st):      # not the legacy default stream: it would wait for every lane
-            host = {k: v.cpu().numpy() for k, v in out.items()}
-        for i, r in enumerate(reqs):
-            r.result = {"Y": host["Y"][:, i].copy(), "T": float(host["T"][i]), "t_ign": float(host["t_ign"][i]),
-                        "t_end": float(host["t_end"][i]), "nsteps": int(host["nsteps"][i])}
-            r.done = now
 
     # ------------------------------------------------------------------ the loop
     def run(self, requests: List[Request], realtime: bool = True, poll_s: float = 2e-4) -> Dict:
@@ -164,7 +237,6 @@ class Server:
         pending_r: List[Request] = []
         pending_g: List[Request] = []
         active: List[_GridJob] = []
-        batches = [None] * len(self.lanes)
         mem_used = 0
         nxt = 0
         t0 = time.perf_counter()
@@ -178,27 +250,32 @@ class Server:
                 nxt += 1
             progressed = False
             # reactor lanes
-            for ln in range(len(self.lanes)):
-                if batches[ln] is not None and batches[ln][2].query():
-                    self._finish_reactors(batches[ln], clock())
-                    n_done += len(batches[ln][0])
-                    batches[ln] = None
-                    progressed = True
-                if batches[ln] is None and pending_r:
+            for lane in self.lanes:
+                if lane.busy:
+                    k = lane.poll(clock())
+                    n_done += k
+                    progressed |= k > 0
+                if not lane.busy and pending_r:
                     take, pending_r = pending_r[:self.reactor_batch], pending_r[self.reactor_batch:]
-                    batches[ln] = self._launch_reactors(ln, take, clock())
+                    now = clock()
+                    for r in take:
+                        r.admitted = now
+                    lane.launch(take, self.t_max, self.max_steps)
                     progressed = True
             # grid lanes
             still = []
             for job in active:
                 if job.event is None or job.event.query():
-                    if job.steps_done >= job.req.steps:
+                    if job.host is not None:             # results have landed
                         self._finish_grid(job, clock())
                         mem_used -= job.nbytes
                         n_done += 1
                         progressed = True
                         continue
-                    self._advance(job)
+                    if job.steps_done >= job.req.steps:
+                        self._drain_grid(job)
+                    else:
+                        self._advance(job)
                     progressed = True
                 still.append(job)
             active = still
@@ -250,8 +327,8 @@ class Server:
         return self._Shape(nv, nv_aux, nx + 2 * ng, ny + 2 * ng, 1 + 2 * ng, nx, ny, 1)
 
     def close(self):
-        for br in self.lanes:
-            br.close()
+        for lane in self.lanes:
+            lane.br.close()
 
 
 def mixed_requests(n: int, rate: float, seed: int, mech: M.Mechanism, flame_steps: int = 20,

@@ -10,12 +10,14 @@ Method names follow the reference (``update_ghost``, ``compute_aux``,
 from __future__ import annotations
 
 import ctypes as C
-from typing import Optional
+import json
+import os
+from typing import Optional, Sequence
 
 import numpy as np
 import torch
 
-from .native import StxFields, check, load_stx
+from .native import StxFields, StxTuning, check, load_stx
 
 
 def _p(t: Optional[torch.Tensor]):
@@ -24,7 +26,11 @@ def _p(t: Optional[torch.Tensor]):
 
 class Solver:
     def __init__(self, case, device: str = "cuda", w: Optional[torch.Tensor] = None,
-                 w_aux: Optional[torch.Tensor] = None):
+                 w_aux: Optional[torch.Tensor] = None, aux_slots: Optional[Sequence[int]] = None):
+        """case: a Case; w, w_aux: device fields to use in place of the case's host
+        fields.  aux_slots: upload only these (0-based) slots of case.w_aux, the
+        others starting at zero -- for a fresh case only the temperature slot
+        (the Newton iteration's first guess) holds data before eval_aux."""
         if not torch.cuda.is_available():
             raise RuntimeError("the stx solver needs a CUDA device (there is no CPU fallback)")
         self.lib = load_stx()
@@ -40,10 +46,18 @@ class Solver:
               "stx_ctx_create")
         self.ctx = ctx
         nv = case.nv
+        # host fields go up through pinned staging, asynchronously on the current
+        # stream (the kernels that follow on it see them)
+        up = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(self.device, non_blocking=True)
         if w is None:
-            w = torch.from_numpy(case.w).to(self.device)
+            w = up(case.w)
         if w_aux is None:
-            w_aux = torch.from_numpy(case.w_aux).to(self.device)
+            if aux_slots is None:
+                w_aux = up(case.w_aux)
+            else:      # only these slots hold data; the others start at zero
+                w_aux = torch.zeros(case.w_aux.shape, dtype=torch.float64, device=self.device)
+                for j in aux_slots:
+                    w_aux[j].copy_(up(case.w_aux[j]), non_blocking=True)
         self.w = w.contiguous()
         self.w_aux = w_aux.contiguous()
         assert self.w.shape == (nv, case.nzg, case.nyg, case.nxg) and self.w.dtype == torch.float64
@@ -106,6 +120,54 @@ class Solver:
         mode = {"fp64": 0, "mixed": 1}[form]
         check(self.lib.stx_set_precision(self.ctx, mode), "stx_set_precision")
         self.precision = form
+
+    # ------------------------------------------------------------------ tuning
+    def tuning(self) -> dict:
+        """The context's launch choices (stx_get_tuning)."""
+        t = StxTuning()
+        check(self.lib.stx_get_tuning(self.ctx, C.byref(t)), "stx_get_tuning")
+        return _tuning_dict(t)
+
+    def set_tuning(self, tune: dict):
+        t = StxTuning()
+        t.sweep_kind[:] = tune["sweep_kind"]
+        t.weno_list[:] = tune["weno_list"]
+        t.chem_ctas_per_sm = tune["chem_ctas_per_sm"]
+        check(self.lib.stx_set_tuning(self.ctx, C.byref(t)), "stx_set_tuning")
+
+    def tuning_key(self) -> str:
+        c = self.case
+        return (f"{torch.cuda.get_device_name(self.device)}|ns={c.ns}|{c.nx}x{c.ny}x{c.nz}|ep={c.ep_order}|"
+                f"weno={c.weno_scheme}|chem={c.enable_chemistry}/{c.rosenbrock_version}|"
+                f"prec={getattr(self, 'precision', 'fp64')}")
+
+    def autotune(self, dt_chem: Optional[float] = None, cache: Optional[str] = None) -> dict:
+        """Choose the launch shapes by timing them (stx_autotune) on the current
+        fields, which must be prepared (``prepare``); they are not modified.
+        dt_chem: the chemistry window to time (default: half of the current dt,
+        the Strang half step).  cache: a JSON file of earlier choices keyed by
+        device, species count, grid, scheme and precision; a hit applies the
+        stored choice without timing, a miss times and adds it."""
+        key = self.tuning_key()
+        if cache and os.path.exists(cache):
+            with open(cache) as fh:
+                known = json.load(fh)
+            if key in known:
+                self.set_tuning(known[key])
+                return dict(known[key], cached=True)
+        t = StxTuning()
+        dtc = 0.5 * self.dt if dt_chem is None else dt_chem
+        check(self.lib.stx_autotune(self.ctx, self.stream, C.byref(self.fields), dtc, C.byref(t)), "stx_autotune")
+        out = _tuning_dict(t)
+        if cache:
+            known = {}
+            if os.path.exists(cache):
+                with open(cache) as fh:
+                    known = json.load(fh)
+            known[key] = out
+            with open(cache, "w") as fh:
+                json.dump(known, fh, indent=1, sort_keys=True)
+        return dict(out, cached=False)
 
     def aux_slot(self, j: int) -> C.c_void_p:
         return C.c_void_p(self.w_aux[j].data_ptr())
@@ -172,3 +234,9 @@ class Solver:
 
     def host_w_aux(self) -> np.ndarray:
         return self.w_aux.cpu().numpy()
+
+
+def _tuning_dict(t: StxTuning) -> dict:
+    return {"sweep_kind": list(t.sweep_kind), "weno_list": list(t.weno_list), "chem_ctas_per_sm": t.chem_ctas_per_sm,
+            "chem_ctas_max": t.chem_ctas_max, "sweep_ms": [round(x, 4) for x in t.sweep_ms],
+            "chem_ms": round(t.chem_ms, 4)}
