@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer leg (default: --steps)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
-    ap.add_argument("--workload", default="turbulence", choices=["turbulence", "reactors", "flame", "serve"],
+    ap.add_argument("--stiff-n", type=int, default=16, help="box edge of --workload stiff53")
+    ap.add_argument("--workload", default="turbulence", choices=["turbulence", "reactors", "flame", "serve", "stiff53"],
                     help="turbulence: the headline reacting-step benchmark; reactors: batched 0-D reactors; "
                          "flame: the 2000-cell 1-D premixed flame of the reference's published timing; "
                          "serve: a Poisson stream of mixed 0-D / 1-D / 2-D solves")
@@ -632,6 +633,118 @@ def run_flame(args):
     return 0
 
 
+# ------------------------------------------------------------------ 53-species stiff mechanism
+def stiff_config(n, world):
+    return {"workload": f"synthetic stiff-mechanism box, {n}^3 cells per GPU: 53 species / 325 seeded reactions "
+                        "(A~logU(1e8,1e16), b~U(-1.5,2), Ea~U(0,50) kcal/mol, 20% third-body), Y~Dirichlet(0.5), "
+                        "T smooth in 1200..2000 K, 1 atm, at rest; WENO5-Z/KEEP(2) hybrid, Strang splitting with the "
+                        "full-Jacobian Rosenbrock (dense 57x57 finite-difference Jacobian and LU per cell), fixed dt "
+                        "1e-10 s",
+            "cells_per_gpu": n ** 3, "species": 53, "reactions": 325, "precision_form": "plain FP64",
+            "parallelism": f"dp{world} (independent boxes)",
+            "size_note": f"{n}^3 stands in for the 128^3 case: at dt 1e-10 s every cell takes thousands of "
+                         "adaptive sub-steps, each with 57 right-hand sides of 325 reactions, so a 128^3 step "
+                         "runs for minutes; the per-cell work does not depend on the box size",
+            "l2": "compute bound (per-cell Jacobian)"}
+
+
+def cpu_stiff(budget_s=20.0):
+    """The oracle on single cells of the same box (one thread per cell), about budget_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from stx import configs
+    from driver import OracleSolver
+    _, tb = configs.stiff_mechanism_tables(0)
+    cores = os.cpu_count() or 1
+    n = 1
+    while True:                                   # grow the sample until it takes a few seconds
+        case = configs.stiff_case(n, seed=3, tables=tb, dt=1e-10)
+        o = OracleSolver(case, threads=cores)
+        o.prepare()
+        t0 = time.perf_counter()
+        o.step()
+        el = time.perf_counter() - t0
+        o.close()
+        if el >= budget_s / 4 or n >= 8 or 8 * el > budget_s:     # the next size costs 8x
+            return n ** 3 / el, cores, f"{n}^3 cells of the same box (seed 3), one step, {el:.1f} s"
+        n *= 2
+
+
+def run_stiff(args):
+    import torch
+    import torch.distributed as dist
+    from stx import configs
+    from stx.solver import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    n = args.stiff_n
+    _, tb = configs.stiff_mechanism_tables(0)
+    sol = Solver(configs.stiff_case(n, seed=3 + rank, tables=tb, dt=1e-10), device=str(dev))
+    sol.prepare()
+    for _ in range(args.warmup):
+        sol.step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        sol.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_max = float(ms.item())
+    value = n ** 3 * world * args.steps / (ms_max / 1e3)
+    # e2e: the state from pinned host memory before and back after every step
+    host_w = torch.empty(sol.w.shape, dtype=torch.float64, pin_memory=True)
+    host_w.copy_(sol.w)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        sol.w.copy_(host_w, non_blocking=True)
+        sol.step()
+        host_w.copy_(sol.w, non_blocking=True)
+    t1.record()
+    torch.cuda.synchronize()
+    ms2 = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms2, op=dist.ReduceOp.MAX)
+    wbytes = sol.w.numel() * 8
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": stiff_config(n, world),
+            "clocks": ck, "gpu_launches": None,
+            "e2e": {"value": n ** 3 * world * args.steps / (float(ms2.item()) / 1e3), "unit": METRIC,
+                    "h2d_bytes_per_step": wbytes, "d2h_bytes_per_step": wbytes,
+                    "path": "Solver.step through the C ABI, state w from pinned host memory before and back after "
+                            "every step"},
+            "status_bits": sol.status()}
+    if world == 1 and rank == 0 and not args.no_cpu:
+        rate, cores, sample = cpu_stiff()
+        line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------------ served mix
 S_METRIC = "solves/s"
 
@@ -699,6 +812,21 @@ def main():
                                       "d2h_bytes_per_step": 0}}), flush=True)
             return 0
         return run_flame(args)
+    if args.workload == "stiff53":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) != 0:
+                return 0
+            rate, cores, sample = cpu_stiff()
+            print(json.dumps({"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC,
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic (seeded)", "config": stiff_config(args.stiff_n, args.gpus),
+                              "cpu_baseline": {"value": rate, "unit": METRIC, "cores": cores, "kind": "port",
+                                               "sample": sample},
+                              "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
+        return run_stiff(args)
     if args.workload == "reactors":
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) != 0:

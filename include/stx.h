@@ -119,6 +119,12 @@ const char *stx_strerror(int code);
  * tables and the grid to device memory, allocates scratch.  Replaces the table
  * upload of multideal_gpu.F90:1361-1424 and the stream set-up of :1468. */
 int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid *grid, stx_ctx **out);
+/* A context for another grid and parameter set on the same mechanism: it uses
+ * base's device tables (no table upload or repacking) and has its own grid,
+ * scratch, counters and status word.  base must outlive every context created
+ * from it.  No counterpart in the reference (one solve per process); for
+ * callers that run many solves of one mechanism, e.g. a request server. */
+int stx_ctx_create_like(const stx_ctx *base, const stx_params *par, const stx_grid *grid, stx_ctx **out);
 int stx_ctx_destroy(stx_ctx *ctx);
 
 /* eval_aux_cuf (kernels_gpu.F90:6154-6308): species clip written back into w,
@@ -247,6 +253,8 @@ typedef struct stx_tuning {
                                 0: computed in line by the sweep */
   int32_t chem_ctas_per_sm;  /* persistent CTAs per SM of the cell chemistry (ROK4); 0: its occupancy limit */
   int32_t chem_ctas_max;     /* out: that occupancy limit */
+  int32_t batch_ctas_max;    /* most CTAs of one stx_batch0d_integrate launch; 0: no cap (a server running
+                                several reactor launches at once caps each, leaving room for other work) */
   float sweep_ms[3];         /* out (stx_autotune): time of the chosen sweep kernels, ms */
   float chem_ms;             /* out (stx_autotune): time of the chosen chemistry launch, ms */
 } stx_tuning;

@@ -172,10 +172,14 @@ int stx_ctx_destroy(stx_ctx *c) {
   return STX_OK;
 }
 
-int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid *grid, stx_ctx **out) {
-  if (!par || !tab || !grid || !out) return STX_E_INVALID;
+}  // extern "C"
+
+// A context from host tables (base null) or on the device tables of base.
+static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const stx_grid *grid, const stx_ctx *base,
+                           stx_ctx **out) {
+  if (!par || !(tab || base) || !grid || !out) return STX_E_INVALID;
   *out = nullptr;
-  const int ns = tab->ns, nr = tab->nr;
+  const int ns = base ? base->ns : tab->ns, nr = base ? base->d.t.nr : tab->nr;
   if (!ns_supported(ns)) return STX_E_UNSUPPORTED;
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || grid->ng < 1 || grid->ng > 4) return STX_E_INVALID;
   if (par->nv_aux < 2 * ns + 13) return STX_E_INVALID;
@@ -194,7 +198,7 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   if (par->eul_imin != 1 || par->eul_imax != grid->nx || par->eul_jmin != 1 || par->eul_jmax != grid->ny ||
       par->eul_kmin != 1 || par->eul_kmax != grid->nz)
     return STX_E_UNSUPPORTED;
-  if (tab->nsetcv < 1 || tab->num_t_tab < 1) return STX_E_INVALID;
+  if (!base && (tab->nsetcv < 1 || tab->num_t_tab < 1)) return STX_E_INVALID;
   if (par->enable_chemistry > 0 && nr < 1) return STX_E_INVALID;
   stx_ctx *c = new (std::nothrow) stx_ctx();
   if (!c) return STX_E_NOMEM;
@@ -213,7 +217,10 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   DevPar &p = d.p;
   int rc = STX_OK;
   auto fail = [&](int code) { stx_ctx_destroy(c); return code; };
-  // ---- tables
+  // ---- tables (shared: base's device copies, which base keeps)
+  if (base) {
+    t = base->d.t;
+  } else {
   t.ns = ns; t.nr = nr; t.icl = tab->indx_cp_l; t.icr = tab->indx_cp_r; t.nset = tab->nsetcv; t.ntab = tab->num_t_tab;
   t.ncp = t.icr - t.icl + 3; t.tmin = tab->t_min_tab; t.dtab = tab->dt_tab; t.Ru = tab->R_univ;
   const size_t ntab1 = (size_t)tab->num_t_tab + 1;
@@ -315,20 +322,30 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
     if ((rc = upload(c, tab->beta0, 2, &t.beta0))) return fail(rc);
     if ((rc = upload(c, tab->nainsp, (size_t)ns * t.n_eoi, &t.nainsp))) return fail(rc);
   }
-  // ---- grid
+  }  // host tables
+  // ---- grid: the nine coordinate and metric arrays in one upload
   g.nx = grid->nx; g.ny = grid->ny; g.nz = grid->nz; g.ng = grid->ng;
   g.nxg = g.nx + 2 * g.ng; g.nyg = g.ny + 2 * g.ng; g.nzg = g.nz + 2 * g.ng;
   g.npg = (long long)g.nxg * g.nyg * g.nzg;
   g.npi = (long long)g.nx * g.ny * g.nz;
-  if ((rc = upload(c, grid->x, g.nxg, &g.x))) return fail(rc);
-  if ((rc = upload(c, grid->y, g.nyg, &g.y))) return fail(rc);
-  if ((rc = upload(c, grid->z, g.nzg, &g.z))) return fail(rc);
-  if ((rc = upload(c, grid->dcsidx, g.nx, &g.dcsidx))) return fail(rc);
-  if ((rc = upload(c, grid->detady, g.ny, &g.detady))) return fail(rc);
-  if ((rc = upload(c, grid->dzitdz, g.nz, &g.dzitdz))) return fail(rc);
-  if ((rc = upload(c, grid->dcsidxs, g.nx, &g.dcsidxs))) return fail(rc);
-  if ((rc = upload(c, grid->detadys, g.ny, &g.detadys))) return fail(rc);
-  if ((rc = upload(c, grid->dzitdzs, g.nz, &g.dzitdzs))) return fail(rc);
+  {
+    const double *src[9] = {grid->x, grid->y, grid->z, grid->dcsidx, grid->detady, grid->dzitdz,
+                            grid->dcsidxs, grid->detadys, grid->dzitdzs};
+    const size_t len[9] = {(size_t)g.nxg, (size_t)g.nyg, (size_t)g.nzg, (size_t)g.nx, (size_t)g.ny,
+                           (size_t)g.nz, (size_t)g.nx, (size_t)g.ny, (size_t)g.nz};
+    size_t off[9], tot = 0;
+    for (int q = 0; q < 9; q++) {
+      off[q] = tot;
+      tot += len[q];
+    }
+    std::vector<double> gb(tot, 0.0);            // an absent array reads as zeros
+    for (int q = 0; q < 9; q++)
+      if (src[q]) std::memcpy(gb.data() + off[q], src[q], len[q] * sizeof(double));
+    const double *gd = nullptr;
+    if ((rc = upload(c, gb.data(), tot, &gd))) return fail(rc);
+    const double **dst[9] = {&g.x, &g.y, &g.z, &g.dcsidx, &g.detady, &g.dzitdz, &g.dcsidxs, &g.detadys, &g.dzitdzs};
+    for (int q = 0; q < 9; q++) *dst[q] = gd + off[q];
+  }
   // ---- numerics
   p.p0 = par->p0; p.rho0 = par->rho0; p.u0 = par->u0; p.eps_sensor = par->eps_sensor; p.tol = par->tol_iter_nr;
   p.sensor_threshold = par->sensor_threshold; p.ros_eps = par->ros_eps;
@@ -369,6 +386,7 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   }
   c->par.winf = nullptr;
   if ((rc = launch_euler_setup(ns))) return fail(rc);
+  if ((rc = launch_batch0d_setup(ns))) return fail(rc);
   for (int q = 0; q < 3; q++) c->weno_list[q] = 1;
   c->weno = WenoScratch{nullptr, nullptr, nullptr, 0};
   const char *wl_env = std::getenv("STX_WENO_LIST");
@@ -389,6 +407,18 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
   if (cudaStreamSynchronize(c->cs) != cudaSuccess) return fail(STX_E_CUDA);
   *out = c;
   return STX_OK;
+}
+
+extern "C" {
+
+int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid *grid, stx_ctx **out) {
+  if (!tab) return STX_E_INVALID;
+  return ctx_create_impl(par, tab, grid, nullptr, out);
+}
+
+int stx_ctx_create_like(const stx_ctx *base, const stx_params *par, const stx_grid *grid, stx_ctx **out) {
+  if (!base) return STX_E_INVALID;
+  return ctx_create_impl(par, nullptr, grid, base, out);
 }
 
 // ------------------------------------------------------------------ aux
@@ -789,6 +819,7 @@ int stx_get_tuning(stx_ctx *c, stx_tuning *out) {
   }
   out->chem_ctas_per_sm = c->d.p.chem_ctas_per_sm;
   out->chem_ctas_max = chem_ctas_limit(c->ns);
+  out->batch_ctas_max = c->d.p.batch_ctas_max;
   return STX_OK;
 }
 
@@ -797,12 +828,13 @@ int stx_set_tuning(stx_ctx *c, const stx_tuning *t) {
   for (int q = 0; q < 3; q++)
     if ((t->sweep_kind[q] != 0 && t->sweep_kind[q] != 1) || (t->weno_list[q] != 0 && t->weno_list[q] != 1))
       return STX_E_INVALID;
-  if (t->chem_ctas_per_sm < 0) return STX_E_INVALID;
+  if (t->chem_ctas_per_sm < 0 || t->batch_ctas_max < 0) return STX_E_INVALID;
   for (int q = 0; q < 3; q++) {
     c->d.p.sweep_kind[q] = t->sweep_kind[q];
     c->weno_list[q] = t->weno_list[q];
   }
   c->d.p.chem_ctas_per_sm = t->chem_ctas_per_sm;
+  c->d.p.batch_ctas_max = t->batch_ctas_max;
   STX_CUDA_TRY(cudaMemcpyAsync((void *)c->dctx_d, &c->d, sizeof(DevCtx), cudaMemcpyHostToDevice, c->cs));
   STX_CUDA_TRY(cudaStreamSynchronize(c->cs));
   return STX_OK;
@@ -843,7 +875,9 @@ int stx_autotune(stx_ctx *c, void *sv, const stx_fields *f, double dt_chem, stx_
         return launch_euler(c->d, c->dctx_d, s, d, f->w_aux, fls, 1, nsw[d], 1, wsc);
       });
       if (ms < 0.f) { rc = STX_E_CUDA; break; }
-      if (best < 0.f || ms < best) { best = ms; pick = k; }
+      // the default (first) stays unless another is clearly faster: the Ducros
+      // sensor marks more faces as the flow develops, which favours the default
+      if (best < 0.f || ms < 0.9f * best) { best = ms; pick = k; }
     }
     c->d.p.sweep_kind[d] = pick.kind;
     c->weno_list[d] = pick.list;
@@ -858,7 +892,7 @@ int stx_autotune(stx_ctx *c, void *sv, const stx_fields *f, double dt_chem, stx_
       const int lim = chem_ctas_limit(c->ns);
       float best = -1.f;
       int pick = 0;
-      for (int k = 1; k <= lim && rc == STX_OK; k++) {
+      for (int k = lim; k >= 1 && rc == STX_OK; k--) {     // the default (the limit) first
         c->d.p.chem_ctas_per_sm = k;
         float ms = time_launches(s, e0, e1, 1, [&] {
           if (cudaMemcpyAsync(w2, f->w, nw * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
@@ -866,7 +900,7 @@ int stx_autotune(stx_ctx *c, void *sv, const stx_fields *f, double dt_chem, stx_
           return launch_rok4(c->d, s, w2, f->w_aux, nullptr, dt_chem, 0.0, dt_chem, 0, c->counter_d);
         });
         if (ms < 0.f) { rc = STX_E_CUDA; break; }
-        if (best < 0.f || ms < best) { best = ms; pick = k; }
+        if (best < 0.f || ms < 0.95f * best) { best = ms; pick = k; }
       }
       c->d.p.chem_ctas_per_sm = pick == lim ? 0 : pick;
       chem_ms = best;

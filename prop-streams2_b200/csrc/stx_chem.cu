@@ -382,6 +382,7 @@ static int batch0d_t(const DevCtx &c, cudaStream_t s, int n, const double *T0, c
   int nb = persistent_blocks((const void *)k_batch0d<NS>, chem_block(NS));
   long long need = ((long long)n + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
+  if (c.p.batch_ctas_max > 0 && nb > c.p.batch_ctas_max) nb = c.p.batch_ctas_max;
   k_batch0d<NS><<<nb, chem_block(NS), 0, s>>>(c, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps,
                                               counter);
   STX_CUDA_TRY(cudaGetLastError());
@@ -396,6 +397,17 @@ int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, con
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;
+  }
+}
+
+// the thread-per-reactor kernel's shared-memory split (see launch_batch0d_setup)
+void batch0d_thread_carveout(int ns) {
+  switch (ns) {
+#define X(N) case N: cudaFuncSetAttribute(k_batch0d<N>, cudaFuncAttributePreferredSharedMemoryCarveout, \
+                                          (int)cudaSharedmemCarveoutMaxShared); break;
+    STX_FOR_NS(X)
+#undef X
+    default: break;
   }
 }
 

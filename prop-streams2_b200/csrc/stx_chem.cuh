@@ -4,12 +4,14 @@
 #pragma once
 #include "stx_kernels.cuh"
 
-// Linkage of the ROK4 right-hand side.  Inlined at its three call sites
-// (default) it avoids the call's register saves and halves the local-memory
-// frame (2.2 KB instead of 3.9 KB per thread); measured 10 % faster than one
-// out-of-line copy now that the production rates are compact.
+// Linkage of the ROK4 right-hand side: one out-of-line copy (default).  Inlined
+// at its three call sites it halves the local-memory frame (2.2 KB instead of
+// 3.9 KB per thread) and is 10 % faster on a fresh field, but on a developed
+// 256^3 reacting field the cells take more sub-steps and the three inlined
+// copies overflow the instruction cache: 306 ms against 178 ms per launch
+// (bit-identical results).
 #ifndef STX_RHS_LINKAGE
-#define STX_RHS_LINKAGE __forceinline__
+#define STX_RHS_LINKAGE __noinline__
 #endif
 
 

@@ -84,6 +84,9 @@ struct DevPar {
   int sweep_kind[3];
   // persistent CTAs per SM of the cell chemistry kernels (0: occupancy limit)
   int chem_ctas_per_sm;
+  // most CTAs of a batched-reactor launch (0: no cap), so that several
+  // concurrent launches leave the SMs room for other work
+  int batch_ctas_max;
 };
 
 struct DevCtx {

@@ -16,6 +16,10 @@
 //    per stencil point instead of O(ns^2).  The back projection keeps the
 //    reference's summation order.  Results equal the reference's dense
 //    products up to rounding.
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "stx_kernels.cuh"
 
 // wenorec_1d / wenorec_1d_rusanov (kernels_gpu.F90:2065-2637) for one variable;
@@ -1088,13 +1092,25 @@ static int euler_setup_t() {
   return STX_OK;
 }
 
+// once per device and species count: the attribute stays with the function for
+// the life of the process, and setting it again is not free while other work
+// runs (contexts are created while a server's solves are in flight)
 int launch_euler_setup(int ns) {
+  static std::mutex mu;
+  static std::set<std::pair<int, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, ns})) return STX_OK;
+  int rc = STX_E_UNSUPPORTED;
   switch (ns) {
-#define X(N) case N: return euler_setup_t<N>();
+#define X(N) case N: rc = euler_setup_t<N>(); break;
     STX_FOR_NS(X)
 #undef X
-    default: return STX_E_UNSUPPORTED;
+    default: break;
   }
+  if (rc == STX_OK) done.insert({dev, ns});
+  return rc;
 }
 
 int launch_euler(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int dir, const double *wa, double *fl, int nmin,

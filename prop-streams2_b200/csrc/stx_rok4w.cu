@@ -19,6 +19,10 @@
 // The dot products are summed in a different order than the sequential loops
 // of the reference (rounding-level differences).  Compiled without FMA
 // contraction, like the other chemistry kernels.
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "stx_chem.cuh"
 
 #define WFULL 0xffffffffu
@@ -325,11 +329,43 @@ static int batch0d_w_t(const DevCtx &c, cudaStream_t s, int n, const double *T0,
   if (!force && need > nb) return STX_E_UNSUPPORTED;
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
   if (nb > need) nb = need;
+  if (c.p.batch_ctas_max > 0 && nb > c.p.batch_ctas_max) nb = c.p.batch_ctas_max;   // after the choice of kernel
   k_batch0d_w<NS><<<(int)nb, 128, 0, s>>>(c, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps,
                                           counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
   }
+}
+
+// The batched-reactor kernels are persistent and can stay resident for seconds.
+// An SM holding one of their CTAs keeps its shared-memory/L1 split until the CTA
+// exits, and a kernel that needs a larger shared-memory share (the staged
+// convective sweeps, ~90 KB per CTA) cannot start a CTA there meanwhile; on a
+// server that runs grid solves beside reactor launches those solves then wait
+// for the reactors.  So the reactor kernels ask for the largest shared-memory
+// split, which every other kernel fits beside.
+template <int NS>
+static void batch0d_carveout_t() {
+  cudaFuncSetAttribute(k_batch0d_w<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
+}
+
+int launch_batch0d_setup(int ns) {
+  static std::mutex mu;
+  static std::set<std::pair<int, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, ns})) return STX_OK;
+  switch (ns) {
+#define X(N) case N: batch0d_carveout_t<N>(); break;
+    STX_FOR_NS(X)
+#undef X
+    default: break;
+  }
+  batch0d_thread_carveout(ns);
+  done.insert({dev, ns});
+  return cudaGetLastError() == cudaSuccess ? STX_OK : STX_E_CUDA;
 }
 
 int launch_batch0d_warp(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,

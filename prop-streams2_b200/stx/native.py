@@ -74,7 +74,8 @@ class StxKprof(C.Structure):
 
 class StxTuning(C.Structure):
     _fields_ = [("sweep_kind", C.c_int32 * 3), ("weno_list", C.c_int32 * 3), ("chem_ctas_per_sm", C.c_int32),
-                ("chem_ctas_max", C.c_int32), ("sweep_ms", C.c_float * 3), ("chem_ms", C.c_float)]
+                ("chem_ctas_max", C.c_int32), ("batch_ctas_max", C.c_int32), ("sweep_ms", C.c_float * 3),
+                ("chem_ms", C.c_float)]
 
 
 _VP = C.c_void_p
@@ -86,6 +87,7 @@ STX_SIGNATURES = [
     ("stx_abi_version", C.c_int, []),
     ("stx_strerror", C.c_char_p, [_I]),
     ("stx_ctx_create", _I, [C.POINTER(StxParams), C.POINTER(StxTables), C.POINTER(StxGrid), C.POINTER(_VP)]),
+    ("stx_ctx_create_like", _I, [_VP, C.POINTER(StxParams), C.POINTER(StxGrid), C.POINTER(_VP)]),
     ("stx_ctx_destroy", _I, [_VP]),
     ("stx_eval_aux", _I, [_VP, _VP, _VP, _VP, _I, _I, _I, _I, _I, _I]),
     ("stx_compute_aux", _I, [_VP, _VP, _VP, _VP, _I, _I]),

@@ -128,6 +128,16 @@ class BatchReactors:
                                              vp(out["t_ign"]), vp(out["t_end"]), vp(out["nsteps"])),
               "stx_batch0d_integrate")
 
+    def set_launch_cap(self, ctas: int):
+        """Cap the CTAs of this context's launches (0: none), so that several
+        reactor launches running at once leave SMs for other work: the
+        persistent kernels hold their CTAs until the last reactor is done."""
+        from .native import StxTuning
+        t = StxTuning()
+        check(self.lib.stx_get_tuning(self.ctx, C.byref(t)), "stx_get_tuning")
+        t.batch_ctas_max = int(ctas)
+        check(self.lib.stx_set_tuning(self.ctx, C.byref(t)), "stx_set_tuning")
+
     def status(self, reset: bool = True) -> int:
         bits = C.c_uint32()
         check(self.lib.stx_status(self.ctx, self.stream(), C.byref(bits), int(reset)), "stx_status")

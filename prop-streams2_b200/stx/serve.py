@@ -68,6 +68,7 @@ class _GridJob:
         self.steps_done = 0
         self.event: Optional[torch.cuda.Event] = None
         self.host: Optional[dict] = None      # pinned result buffers while draining
+        self.graph = None                     # captured chunk of steps
 
 
 class _ReactorLane:
@@ -139,7 +140,7 @@ class Server:
     every served batch, like a request served alone, takes that kernel)."""
 
     def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 32, chunk: int = 5,
-                 reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 4):
+                 reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 16):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -148,6 +149,12 @@ class Server:
         self.lanes = [_ReactorLane(BatchReactors("h2air_9sp", device=str(self.device), tables=rtab),
                                    torch.cuda.Stream(self.device), reactor_batch) for _ in range(reactor_lanes)]
         self.reactors = self.lanes[0].br
+        # the lanes' persistent kernels together hold at most one CTA per SM
+        # (half the warp kernel's occupancy), so the grid solves' kernels keep
+        # finding room on every SM
+        nsm = torch.cuda.get_device_properties(self.device).multi_processor_count
+        for lane in self.lanes:
+            lane.br.set_launch_cap(max(2, nsm // reactor_lanes))
         self.tables = {
             "flame1d": M.build_tables(configs.mechanism("h2air_9sp"), 101325.0, 200.0, 5500.0, 1.0),
             "tube2d": M.build_tables(configs.mechanism("shock_tube_9sp"), 7173.0, 200.0, 20000.0, 1.0),
@@ -155,6 +162,14 @@ class Server:
         self.mem_budget, self.max_grid, self.chunk = mem_budget, max_grid, chunk
         self.reactor_batch, self.t_max, self.max_steps = reactor_batch, t_max, max_steps
         self._cases: Dict[tuple, object] = {}
+        # one small solver per grid kind holds that mechanism's device tables;
+        # every request's context shares them (stx_ctx_create_like): admitting a
+        # request uploads its fields and grid only
+        self._bases = {
+            "flame1d": Solver(configs.flame_case(64, tables=self.tables["flame1d"], mech_name="h2air_9sp"),
+                              device=str(self.device)),
+            "tube2d": Solver(configs.tube_case(16, 4, tables=self.tables["tube2d"]), device=str(self.device)),
+        }
 
     # ------------------------------------------------------------------ grid solves
     def _case(self, req: Request):
@@ -188,16 +203,25 @@ class Server:
         stream = torch.cuda.Stream(self.device)
         with torch.cuda.stream(stream):
             # a fresh case's w_aux holds only the temperature guess
-            sol = Solver(case, device=str(self.device), aux_slots=(case.J("T"),))
+            sol = Solver(case, device=str(self.device), aux_slots=(case.J("T"),), tables_from=self._bases[req.kind])
             sol.prepare()
         req.admitted = now
         return _GridJob(req, sol, stream, self.grid_bytes(case))
 
     def _advance(self, job: _GridJob):
+        """Enqueue the job's next chunk of steps: a replay of its captured graph of
+        `chunk` steps (fixed dt: bit-identical to the steps one by one), or, for
+        a shorter remainder, the steps one by one."""
         n = min(self.chunk, job.req.steps - job.steps_done)
         with torch.cuda.stream(job.stream):
-            for _ in range(n):
-                job.sol.step()
+            c = job.sol.case
+            if n == self.chunk and c.cfl < 0 and c.iter_dt_recompute == 1:
+                if job.graph is None:
+                    job.graph = job.sol.capture(self.chunk)
+                job.sol.replay(job.graph)
+            else:
+                for _ in range(n):
+                    job.sol.step()
             job.event = torch.cuda.Event()
             job.event.record(job.stream)
         job.steps_done += n
@@ -329,6 +353,8 @@ class Server:
     def close(self):
         for lane in self.lanes:
             lane.br.close()
+        for b in self._bases.values():
+            b.close()
 
 
 def mixed_requests(n: int, rate: float, seed: int, mech: M.Mechanism, flame_steps: int = 20,

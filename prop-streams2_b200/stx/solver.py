@@ -26,11 +26,14 @@ def _p(t: Optional[torch.Tensor]):
 
 class Solver:
     def __init__(self, case, device: str = "cuda", w: Optional[torch.Tensor] = None,
-                 w_aux: Optional[torch.Tensor] = None, aux_slots: Optional[Sequence[int]] = None):
+                 w_aux: Optional[torch.Tensor] = None, aux_slots: Optional[Sequence[int]] = None,
+                 tables_from: Optional["Solver"] = None):
         """case: a Case; w, w_aux: device fields to use in place of the case's host
         fields.  aux_slots: upload only these (0-based) slots of case.w_aux, the
         others starting at zero -- for a fresh case only the temperature slot
-        (the Newton iteration's first guess) holds data before eval_aux."""
+        (the Newton iteration's first guess) holds data before eval_aux.
+        tables_from: a live solver of the same mechanism whose device tables
+        this one uses (stx_ctx_create_like); it must outlive this one."""
         if not torch.cuda.is_available():
             raise RuntimeError("the stx solver needs a CUDA device (there is no CPU fallback)")
         self.lib = load_stx()
@@ -42,8 +45,14 @@ class Solver:
         torch.cuda.set_device(self.device)
         self._par, self._tab, self._grid = case.params_struct(), case.tables_struct(), case.grid_struct()
         ctx = C.c_void_p()
-        check(self.lib.stx_ctx_create(C.byref(self._par), C.byref(self._tab), C.byref(self._grid), C.byref(ctx)),
-              "stx_ctx_create")
+        if tables_from is not None:
+            if tables_from.case.ns != case.ns or not tables_from.ctx:
+                raise ValueError("tables_from must be a live solver of the same mechanism")
+            check(self.lib.stx_ctx_create_like(tables_from.ctx, C.byref(self._par), C.byref(self._grid), C.byref(ctx)),
+                  "stx_ctx_create_like")
+        else:
+            check(self.lib.stx_ctx_create(C.byref(self._par), C.byref(self._tab), C.byref(self._grid), C.byref(ctx)),
+                  "stx_ctx_create")
         self.ctx = ctx
         nv = case.nv
         # host fields go up through pinned staging, asynchronously on the current
@@ -133,6 +142,7 @@ class Solver:
         t.sweep_kind[:] = tune["sweep_kind"]
         t.weno_list[:] = tune["weno_list"]
         t.chem_ctas_per_sm = tune["chem_ctas_per_sm"]
+        t.batch_ctas_max = tune.get("batch_ctas_max", 0)
         check(self.lib.stx_set_tuning(self.ctx, C.byref(t)), "stx_set_tuning")
 
     def tuning_key(self) -> str:
@@ -238,5 +248,6 @@ class Solver:
 
 def _tuning_dict(t: StxTuning) -> dict:
     return {"sweep_kind": list(t.sweep_kind), "weno_list": list(t.weno_list), "chem_ctas_per_sm": t.chem_ctas_per_sm,
-            "chem_ctas_max": t.chem_ctas_max, "sweep_ms": [round(x, 4) for x in t.sweep_ms],
+            "chem_ctas_max": t.chem_ctas_max, "batch_ctas_max": t.batch_ctas_max,
+            "sweep_ms": [round(x, 4) for x in t.sweep_ms],
             "chem_ms": round(t.chem_ms, 4)}

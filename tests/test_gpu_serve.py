@@ -72,3 +72,23 @@ def test_memory_budget_limits_admission():
             assert np.array_equal(r.result["w"], reqs[0].result["w"])
     finally:
         srv.close()
+
+
+def test_context_on_shared_tables_equals_a_fresh_one():
+    """stx_ctx_create_like: a solver on another solver's device tables gives the
+    same fields, bit for bit, as one that uploaded its own."""
+    from stx import mech as M
+    from stx.solver import Solver
+    tb = M.build_tables(configs.mechanism("h2air_9sp"), 101325.0, 200.0, 5500.0, 1.0)
+    base = Solver(configs.flame_case(64, tables=tb, mech_name="h2air_9sp"))
+    make = lambda: configs.flame_case(300, phi=0.9, Tu=450.0, tables=tb, mech_name="h2air_9sp")
+    out = []
+    for kw in ({}, {"tables_from": base}):
+        s = Solver(make(), **kw)
+        s.prepare()
+        for _ in range(3):
+            s.step()
+        out.append(s.host_w())
+        s.close()
+    base.close()
+    assert np.array_equal(out[0], out[1])
