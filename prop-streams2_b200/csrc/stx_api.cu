@@ -231,6 +231,21 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   if ((rc = upload(c, tab->cp_coeff, (size_t)t.ncp * ns * t.nset, &t.cp))) return fail(rc);
   if ((rc = upload(c, tab->cv_coeff, (size_t)t.ncp * ns * t.nset, &t.cv))) return fail(rc);
   {
+    // integrated tables: coef_l / (l + 1) for the terms l >= 0 of h(T) and e(T)
+    // (the quotient the reference forms per evaluation, get_species_h_from_temperature_dev)
+    const size_t ncoef = (size_t)t.ncp * ns * t.nset;
+    std::vector<double> hi(tab->cp_coeff, tab->cp_coeff + ncoef), ei(tab->cv_coeff, tab->cv_coeff + ncoef);
+    for (size_t q = 0; q < ncoef; q++) {
+      const int l = t.icl + (int)(q % (size_t)t.ncp);
+      if (l >= 0 && l <= t.icr) {
+        hi[q] = tab->cp_coeff[q] / (l + 1.0);
+        ei[q] = tab->cv_coeff[q] / (l + 1.0);
+      }
+    }
+    if ((rc = upload(c, hi.data(), ncoef, &t.cpi))) return fail(rc);
+    if ((rc = upload(c, ei.data(), ncoef, &t.cvi))) return fail(rc);
+  }
+  {
     // repack the 1-K tables row-major in temperature so one point reads two contiguous rows
     std::vector<double> vr(ntab1 * ns), lr(ntab1 * ns), dr(ntab1 * ns * ns);
     for (size_t it = 0; it < ntab1; it++)

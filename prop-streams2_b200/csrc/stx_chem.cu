@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
     const double T0r = T0[r];
     double h = 0.0;
 #pragma unroll 1
-    for (int k = 0; k < NS; k++) h = h + VEC[k] * species_poly_int(c.t, c.t.cp, T0r, k + 1);
+    for (int k = 0; k < NS; k++) h = h + VEC[k] * species_poly_int(c.t, c.t.cpi, T0r, k + 1);
     Rok4ConstP<NS> f{c, h, p0[r], T0r, ign_factor, end_factor, -1.0, 0.0, T0r, 0};
     rok4_core<NS>(c, f, VEC, T0r, nullptr, dttry, 0.0, t_max, 0);
 #pragma unroll

@@ -30,6 +30,7 @@ struct DevTab {
   const double *mw, *mwinv, *rgas;
   const double *trange;           // (ns, nset+1)
   const double *cp, *cv;          // (ncp, ns, nset)
+  const double *cpi, *cvi;        // the same with coef_l / (l + 1) for l >= 0 (species_poly_int)
   const double *visc_r, *lam_r;   // repacked [it][lsp]
   const double *diff_r;           // repacked [it][lsp][msp] (msp fastest)
   const int *reac_ty, *is_rev;
@@ -153,8 +154,16 @@ __device__ double mix_cp(const DevTab &t, double tt, const double *Y) {
     for (int k = 0; k < NS; k++) nrange[k] = locate_range(t, tt, k + 1);
   }
   double cploc = 0.0;
+  double pw = 1.0;                       // tt^pe: ipow's partial products, formed once
+  int pe = 0;
   for (int l = t.icl; l <= t.icr; l++) {
-    double tpow = ipow(tt, l);
+    double tpow;
+    if (l >= 0) {
+      while (pe < l) { pw = pw * tt; pe++; }
+      tpow = pw;
+    } else {
+      tpow = ipow(tt, l);
+    }
     double cp_l = 0.0;
 #pragma unroll
     for (int k = 0; k < NS; k++) cp_l = cp_l + cpc(t, t.cp, l, k + 1, nrange[k]) * Y[k];
@@ -202,14 +211,25 @@ __device__ double temp_from_poly(const DevTab &t, const double *coef, const DevP
     for (int k = 0; k < NS; k++) sumb = sumb + cpc(t, coef, t.icr + 1, k + 1, nrange[k]) * Y[k];
     double ebar = ee - sumb;
     double den = 0.0, num = 0.0;
+    double pw = 1.0;                     // T_old^pe: ipow's partial products, formed once
+    int pe = 0;
     for (int l = t.icl; l <= t.icr; l++) {
-      double T_pow = ipow(T_old, l);
+      double T_pow;
+      if (l >= 0) {
+        while (pe < l) { pw = pw * T_old; pe++; }
+        T_pow = pw;
+      } else {
+        T_pow = ipow(T_old, l);
+      }
       double tden = T_pow, tnum;
       if (l == -1) {
         tnum = log(T_old);
       } else {
         double T_powp = T_old * T_pow;
-        tnum = T_powp / (l + 1.0);
+        // T_powp / (l + 1): a division by 1, 2 or 4 is an exact scaling (the
+        // same result as the division), the others are divisions
+        const int d = l + 1;
+        tnum = d == 1 ? T_powp : (d == 2 ? T_powp * 0.5 : (d == 4 ? T_powp * 0.25 : T_powp / (l + 1.0)));
       }
       double cv_l = 0.0;
 #pragma unroll
@@ -225,14 +245,27 @@ __device__ double temp_from_poly(const DevTab &t, const double *coef, const DevP
   return tt;
 }
 
-// get_species_h/e_from_temperature_dev (kernels_gpu.F90:7104-7183)
-__device__ __forceinline__ double species_poly_int(const DevTab &t, const double *arr, double tt, int isp) {
+// get_species_h/e_from_temperature_dev (kernels_gpu.F90:7104-7183).  ai is the
+// integrated table (DevTab::cpi / cvi): entry l holds coef_l / (l + 1), the
+// quotient the reference forms for every term, formed once at context creation
+// (the same correctly rounded division, so the same bits).  The powers T^(l+1)
+// for l + 1 >= 1 are formed incrementally, T^(n+1) = T^n * T, the very products
+// of the repeated multiplication ipow performs.
+__device__ __forceinline__ double species_poly_int(const DevTab &t, const double *ai, double tt, int isp) {
   int nr = 1;
   if (t.nset > 1) nr = locate_range(t, tt, isp);
-  double hh = cpc(t, arr, t.icr + 1, isp, nr);
+  double hh = cpc(t, ai, t.icr + 1, isp, nr);
+  double tp = 1.0;                       // tt^tpe, ipow's partial products
+  int tpe = 0;
   for (int l = t.icl; l <= t.icr; l++) {
-    if (l == -1) hh = hh + cpc(t, arr, l, isp, nr) * log(tt);
-    else hh = hh + cpc(t, arr, l, isp, nr) / (l + 1.0) * ipow(tt, l + 1);
+    if (l == -1) {
+      hh = hh + cpc(t, ai, l, isp, nr) * log(tt);
+    } else if (l + 1 >= 1) {
+      while (tpe < l + 1) { tp = tp * tt; tpe++; }
+      hh = hh + cpc(t, ai, l, isp, nr) * tp;
+    } else {
+      hh = hh + cpc(t, ai, l, isp, nr) * ipow(tt, l + 1);
+    }
   }
   return hh;
 }

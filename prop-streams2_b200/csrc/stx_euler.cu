@@ -320,7 +320,7 @@ __device__ __forceinline__ void roe_state(const DevCtx &c, const double *__restr
   double p_e = rho * gm1loc;
 #pragma unroll
   for (int k = 0; k < NS; k++) {
-    double eei = species_poly_int(t, t.cv, tt, k + 1);
+    double eei = species_poly_int(t, t.cvi, tt, k + 1);
     prhoi[k] = ldg(t.rgas + k) * tt + gm1loc * (ee - eei);
   }
   double etot = ee + qq;
@@ -720,17 +720,36 @@ __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? 4 : 2)
   // x: rows r = blockIdx.x * NL + l over (j, k); y: i = blockIdx.x NL + l + 1, k = blockIdx.z + 1;
   // z: i = blockIdx.x NL + l + 1, j = blockIdx.z + 1
   const long long st = DIR == 0 ? 1LL : (DIR == 1 ? (long long)g.nxg : (long long)g.nxg * g.nyg);
-  auto line_base = [&](int l, bool &act) -> long long {   // gidx of the cell at sweep coordinate 0
+  // per line: ghosted index of its cell at sweep coordinate 0 (-1: no such
+  // line) and interior index of its cell at sweep coordinate 0, formed once
+  // (x: rows r = blockIdx.x NL + l over (j, k); y / z: i = blockIdx.x NL + l + 1
+  // with k resp. j = blockIdx.z + 1)
+  __shared__ long long s_gb[NL], s_fb[NL];
+  if (t < NL) {
+    const int l = t;
+    long long gb = -1, fb = 0;
     if (DIR == 0) {
       long long r = (long long)blockIdx.x * NL + l;
-      act = r < (long long)g.ny * g.nz;
-      int j = 1 + (int)(r % g.ny), k = 1 + (int)(r / g.ny);
-      return act ? gidx(g, 0, j, k) : 0;
+      if (r < (long long)g.ny * g.nz) {
+        int j = 1 + (int)(r % g.ny), k = 1 + (int)(r / g.ny);
+        gb = gidx(g, 0, j, k);
+        fb = fidx(g, 0, j, k);
+      }
     } else {
       int i = blockIdx.x * NL + l + 1;
-      act = i <= g.nx;
-      return act ? (DIR == 1 ? gidx(g, i, 0, blockIdx.z + 1) : gidx(g, i, blockIdx.z + 1, 0)) : 0;
+      if (i <= g.nx) {
+        gb = DIR == 1 ? gidx(g, i, 0, blockIdx.z + 1) : gidx(g, i, blockIdx.z + 1, 0);
+        fb = DIR == 1 ? fidx(g, i, 0, blockIdx.z + 1) : fidx(g, i, blockIdx.z + 1, 0);
+      }
     }
+    s_gb[l] = gb;
+    s_fb[l] = fb;
+  }
+  __syncthreads();
+  auto line_base = [&](int l, bool &act) -> long long {
+    const long long gb = s_gb[l];
+    act = gb >= 0;
+    return gb;
   };
   // 1. stage the cells c0-3 .. c0+TC+2 of every line (zero outside the ghosted box)
   for (int e = t; e < NVC * S * NL; e += NT) {
@@ -893,15 +912,8 @@ __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? 4 : 2)
     bool act;
     line_base(l, act);
     if (act && i <= nmax) {
-      long long qf;
-      if (DIR == 0) {
-        long long r = (long long)blockIdx.x * NL + l;
-        qf = fidx(g, i, 1 + (int)(r % g.ny), 1 + (int)(r / g.ny));
-      } else if (DIR == 1) {
-        qf = fidx(g, blockIdx.x * NL + l + 1, i, blockIdx.z + 1);
-      } else {
-        qf = fidx(g, blockIdx.x * NL + l + 1, blockIdx.z + 1, i);
-      }
+      const long long fst = DIR == 0 ? 1LL : (DIR == 1 ? (long long)g.nx : (long long)g.nx * g.ny);
+      const long long qf = s_fb[l] + (long long)i * fst;
       const double *met = DIR == 0 ? g.dcsidx : (DIR == 1 ? g.detady : g.dzitdz);
       double mt = ldg(met + i - 1);
 #pragma unroll

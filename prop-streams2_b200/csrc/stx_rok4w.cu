@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(128) k_batch0d_w(DevCtx c, int n, const double
     const double T0r = T0[r];
     double h = 0.0;
 #pragma unroll 1
-    for (int k = 0; k < NS; k++) h = h + Y0[(long long)k * n + r] * species_poly_int(c.t, c.t.cp, T0r, k + 1);
+    for (int k = 0; k < NS; k++) h = h + Y0[(long long)k * n + r] * species_poly_int(c.t, c.t.cpi, T0r, k + 1);
     Rok4ConstPW<NS> f{c, h, p0[r], T0r, ign_factor, end_factor, sm, -1.0, 0.0, T0r, 0};
     rok4_core_w<NS>(c, f, v, T0r, 0.0, dttry, 0.0, t_max, 0, lane);
     if (lane < NS) Y[(long long)lane * n + r] = v;

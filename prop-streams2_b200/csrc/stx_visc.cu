@@ -61,8 +61,8 @@ __device__ __forceinline__ void visc_face(const DevCtx &c, const double *__restr
     R xxp = yp[k] * mwmp, xx = yl[k] * mwm;
     R sig = -rd[k] * (xxp - xx) * mwmif + fhat_tmp * yyf;
     fh[k] = sig;
-    R hh = have_hl ? hl[k] : (R)species_poly_int(t, t.cp, (double)tt, k + 1);
-    R hhp = (R)species_poly_int(t, t.cp, (double)ttp, k + 1);
+    R hh = have_hl ? hl[k] : (R)species_poly_int(t, t.cpi, (double)tt, k + 1);
+    R hhp = (R)species_poly_int(t, t.cpi, (double)ttp, k + 1);
     hl[k] = hhp;
     R hhf = R(0.5) * (hh + hhp);
     et = et + sig * hhf;

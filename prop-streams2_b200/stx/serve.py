@@ -33,11 +33,18 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import os
 import time
 from typing import Dict, List, Optional
 
 import numpy as np
 import torch
+
+# The server runs tens of streams.  CUDA maps streams onto a few hardware queues
+# (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default), and work queued behind a
+# long-running kernel in one stream then waits in every stream that shares its
+# queue.  32 queues, if CUDA has not been initialised in this process yet.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 from . import configs
 from . import mech as M
@@ -84,7 +91,6 @@ class _ReactorLane:
         self.T, self.t_ign, self.t_end = (torch.empty(cap, **f64) for _ in range(3))
         self.nsteps = torch.empty(cap, dtype=torch.int32, pin_memory=True)
         self.reqs: Optional[List[Request]] = None
-        self.event: Optional[torch.cuda.Event] = None
         self.collected: Optional[np.ndarray] = None
 
     @property
@@ -105,10 +111,13 @@ class _ReactorLane:
         self.nsteps.numpy()[:n] = -1
         out = {"Y": self.Y[:ns * n].view(ns, n), "T": self.T[:n], "t_ign": self.t_ign[:n], "t_end": self.t_end[:n],
                "nsteps": self.nsteps[:n]}
+        # No event behind the launch: an operation queued after a kernel that runs
+        # for seconds would hold up the hardware queue it shares with other
+        # streams.  The lane is free once every reactor has reported (the kernel
+        # reads a reactor's inputs before it writes its step count, so the
+        # buffers may then be refilled; the next launch follows in stream order).
         with torch.cuda.stream(self.stream):
             self.br.launch(self.T0[:n], self.p0[:n], Y0, out, t_max, 1e-8, 1.05, 2.0, max_steps)
-            self.event = torch.cuda.Event()
-            self.event.record(self.stream)
         self.reqs = reqs
         self.collected = np.zeros(n, dtype=bool)
 
@@ -125,7 +134,7 @@ class _ReactorLane:
                                        "t_end": float(te[i]), "nsteps": int(st[i])}
                 self.reqs[i].done = now
             self.collected[fresh] = True
-        if self.collected.all() and self.event.query():
+        if self.collected.all():
             self.reqs = None
         return int(fresh.size)
 
