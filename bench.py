@@ -335,12 +335,13 @@ def run_stx(args):
         with open(peaks_fn) as fh:
             peak = float(json.load(fh)["hbm_gbs"])
         peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
-    traffic = None
-    tfn = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(tfn):
-        with open(tfn) as fh:
-            tr = json.load(fh)
-        traffic = tr.get(dom, {}).get("dram_bytes_per_launch")
+    # DRAM bytes per algorithmic byte of the kernel class, from one ncu capture
+    # at 96^3 (profiles/k_visc_yz_turbulence96_h2air9.md: 363.3 of 354.0 MB;
+    # profiles/k_euler_tile_turbulence96_h2air9.md: 325.7 of 304.3 MB); the
+    # traffic grows in proportion to the cells, so it scales to this launch
+    dram_per_alg = {"visc": 363.3 / 354.0, "euler": 325.7 / 304.3}
+    bpl = cls[dom]["bytes"] / max(1, cls[dom]["launches"])
+    traffic = dram_per_alg[dom] * bpl if dom in dram_per_alg else None
     ach = cls[dom]["gbs"]
     roofline = {"bound": "hbm", "kernel_class": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak if ach else None, "traffic": traffic, "peak_source": peak_src,

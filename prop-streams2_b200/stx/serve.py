@@ -40,11 +40,17 @@ from typing import Dict, List, Optional
 import numpy as np
 import torch
 
-# The server runs tens of streams.  CUDA maps streams onto a few hardware queues
-# (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default), and work queued behind a
-# long-running kernel in one stream then waits in every stream that shares its
-# queue.  32 queues, if CUDA has not been initialised in this process yet.
+# Two process-wide CUDA settings, applied if CUDA has not been initialised in
+# this process yet:
+#  * the server runs tens of streams; CUDA maps streams onto a few hardware
+#    queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default), and work queued behind
+#    a long-running kernel in one stream then waits in every stream that shares
+#    its queue: 32 queues;
+#  * with lazy module loading (the default), the first launch of a kernel (or a
+#    stream capture that includes it) loads it and waits for the running
+#    kernels -- seconds behind a reactor launch: all kernels load at start.
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 
 from . import configs
 from . import mech as M
@@ -76,6 +82,36 @@ class _GridJob:
         self.event: Optional[torch.cuda.Event] = None
         self.host: Optional[dict] = None      # pinned result buffers while draining
         self.graph = None                     # captured chunk of steps
+        self.staged: List[torch.Tensor] = []  # pinned pool buffers in use by the job
+
+
+class _PinnedPool:
+    """Pinned host buffers in power-of-two size classes, kept for reuse.  A new
+    pinned allocation (cudaHostAlloc) can wait for the device to go idle, which
+    on a busy server means waiting for reactor launches that run for seconds;
+    served requests therefore stage their fields through buffers taken from
+    here, and allocations happen only while the pool warms up."""
+
+    def __init__(self):
+        self.free: Dict[int, List[torch.Tensor]] = {}
+
+    def take(self, numel: int) -> torch.Tensor:
+        size = 1 << max(12, (int(numel) - 1).bit_length())
+        lst = self.free.get(size)
+        if lst:
+            return lst.pop()
+        return torch.empty(size, dtype=torch.float64, pin_memory=True)
+
+    def give(self, buf: torch.Tensor):
+        self.free.setdefault(buf.numel(), []).append(buf)
+
+    def warm(self, max_numel: int, per_class: int):
+        """Allocate per_class buffers of every size class up to max_numel."""
+        size = 1 << 12
+        while size <= max_numel:
+            for _ in range(per_class):
+                self.give(torch.empty(size, dtype=torch.float64, pin_memory=True))
+            size <<= 1
 
 
 class _ReactorLane:
@@ -143,13 +179,15 @@ class Server:
     """Continuous-batching server for one GPU.
 
     mem_budget: bytes of HBM the grid solves may hold at once; max_grid: most
-    grid solves in flight; chunk: steps enqueued per grid solve per pass;
+    grid solves in flight; chunk: steps enqueued per grid solve per pass
+    (graphs: as one replay of a captured graph of chunk steps);
     reactor_batch: most reactors per batched launch (the default, 1024, stays
     within the reactors the warp-per-reactor kernel runs at once on a B200, so
     every served batch, like a request served alone, takes that kernel)."""
 
     def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 32, chunk: int = 5,
-                 reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 16):
+                 reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 16,
+                 graphs: bool = True):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -171,6 +209,9 @@ class Server:
         self.mem_budget, self.max_grid, self.chunk = mem_budget, max_grid, chunk
         self.reactor_batch, self.t_max, self.max_steps = reactor_batch, t_max, max_steps
         self._cases: Dict[tuple, object] = {}
+        self.graphs = graphs
+        self.pinned = _PinnedPool()
+        self.pinned.warm(1 << 23, 4)          # up to 64 MB buffers (a 512 x 128 tube's w is 50 MB)
         # one small solver per grid kind holds that mechanism's device tables;
         # every request's context shares them (stx_ctx_create_like): admitting a
         # request uploads its fields and grid only
@@ -210,12 +251,26 @@ class Server:
     def _admit_grid(self, req: Request, now: float) -> _GridJob:
         case = self._case(req)
         stream = torch.cuda.Stream(self.device)
+        staged = []
         with torch.cuda.stream(stream):
-            # a fresh case's w_aux holds only the temperature guess
-            sol = Solver(case, device=str(self.device), aux_slots=(case.J("T"),), tables_from=self._bases[req.kind])
+            # the host fields go up through pinned pool buffers; a fresh case's
+            # w_aux holds only the temperature guess (the rest starts at zero)
+            def up(a):
+                buf = self.pinned.take(a.size)
+                staged.append(buf)
+                v = buf[:a.size].view(a.shape)
+                v.numpy()[...] = a
+                return torch.empty(a.shape, dtype=torch.float64, device=self.device).copy_(v, non_blocking=True)
+            w = up(case.w)
+            w_aux = torch.zeros(case.w_aux.shape, dtype=torch.float64, device=self.device)
+            jT = case.J("T")
+            w_aux[jT].copy_(up(case.w_aux[jT]))
+            sol = Solver(case, device=str(self.device), w=w, w_aux=w_aux, tables_from=self._bases[req.kind])
             sol.prepare()
         req.admitted = now
-        return _GridJob(req, sol, stream, self.grid_bytes(case))
+        job = _GridJob(req, sol, stream, self.grid_bytes(case))
+        job.staged = staged                  # released when the job ends (the copies are done by then)
+        return job
 
     def _advance(self, job: _GridJob):
         """Enqueue the job's next chunk of steps: a replay of its captured graph of
@@ -224,7 +279,7 @@ class Server:
         n = min(self.chunk, job.req.steps - job.steps_done)
         with torch.cuda.stream(job.stream):
             c = job.sol.case
-            if n == self.chunk and c.cfl < 0 and c.iter_dt_recompute == 1:
+            if self.graphs and n == self.chunk and c.cfl < 0 and c.iter_dt_recompute == 1:
                 if job.graph is None:
                     job.graph = job.sol.capture(self.chunk)
                 job.sol.replay(job.graph)
@@ -239,9 +294,11 @@ class Server:
         """Enqueue the result's copies into pinned host buffers (and the status
         word) on the job's stream; the loop completes the job when they land."""
         sol = job.sol
-        h = {"w": torch.empty(sol.w.shape, dtype=torch.float64, pin_memory=True),
-             "T": torch.empty(sol.w_aux.shape[1:], dtype=torch.float64, pin_memory=True),
-             "status": torch.zeros(1, dtype=torch.int32, pin_memory=True)}
+        bw, bt, bs = self.pinned.take(sol.w.numel()), self.pinned.take(sol.w_aux[0].numel()), self.pinned.take(1)
+        job.staged += [bw, bt, bs]
+        h = {"w": bw[:sol.w.numel()].view(sol.w.shape), "T": bt[:sol.w_aux[0].numel()].view(sol.w_aux.shape[1:]),
+             "status": bs[:1].view(torch.int32)[:1]}
+        h["status"].zero_()
         with torch.cuda.stream(job.stream):
             h["w"].copy_(sol.w, non_blocking=True)
             h["T"].copy_(sol.w_aux[sol.case.J("T")], non_blocking=True)
@@ -257,6 +314,9 @@ class Server:
                           "status": int(h["status"].numpy()[0]) & 0xffffffff}
         job.req.done = now
         job.sol.close()
+        for b in job.staged:
+            self.pinned.give(b)
+        job.staged = []
 
     # ------------------------------------------------------------------ the loop
     def run(self, requests: List[Request], realtime: bool = True, poll_s: float = 2e-4) -> Dict:
