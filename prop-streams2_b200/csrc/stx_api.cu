@@ -329,7 +329,6 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
       for (int r = 0; r < nr; r++) kr[it * nr + r] = tab->kc_tab[(size_t)r * ntab1 + it];
     if ((rc = upload(c, kr.data(), kr.size(), &t.kc_r))) return fail(rc);
   }
-  t.fused_arr = arrhenius_form_default();
   t.n_eoi = tab->n_eoi;
   if (t.n_eoi != 1) {
     if (t.n_eoi < 1 || !tab->aw_eoi || !tab->coeff_eoi || !tab->beta0 || !tab->nainsp) return fail(STX_E_INVALID);

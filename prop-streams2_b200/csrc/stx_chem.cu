@@ -11,9 +11,6 @@
 // operations as the reference, so the result is independent of the schedule.
 // This file is compiled without FMA contraction so that its arithmetic matches
 // the FP64 oracle operation by operation (libm vs CUDA exp/pow/log10 aside).
-#include <cstdlib>
-#include <cstring>
-
 #include "stx_chem.cuh"
 
 // CTAs per SM the ROK4 kernel's register budget is sized for
@@ -401,11 +398,6 @@ int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, con
 #undef X
     default: return STX_E_UNSUPPORTED;
   }
-}
-
-int arrhenius_form_default() {
-  const char *e = std::getenv("STX_ARRHENIUS");
-  return (e && std::strcmp(e, "reference") == 0) ? 0 : 1;
 }
 
 // the thread-per-reactor kernel's shared-memory split (see launch_batch0d_setup)

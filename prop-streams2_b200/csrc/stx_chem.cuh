@@ -30,37 +30,19 @@ __device__ __forceinline__ void kc_pos(const DevTab &t, double tt, int &itt, dou
 // table.  KCF selects where K_c is read: false -> t.kc_r, the context's
 // temperature-major repacking; true -> t.kc_r in the reference's own layout
 // kc_tab(num_t_tab+1, nr).
-//
-// Arrhenius form: with t.fused_arr (the default) a modified Arrhenius term with
-// b != 0 is A exp(b ln T - E/(R T)), one exponential with ln T formed once per
-// right-hand side (lnT); otherwise A T^b exp(-E/(R T)) as the reference writes
-// it, a power and an exponential.  The two agree to a few ulps.
-__device__ __forceinline__ double arrhenius(const DevTab &t, double A, double B, double E, double tt, double lnT,
-                                            double Rtti) {
-  if (t.fused_arr && B != 0.0) return A * exp(B * lnT - E * Rtti);
-  double k = A;
-  if (B != 0.0) k = k * pow(tt, B);
-  if (E != 0.0) k = k * exp(-E * Rtti);
-  return k;
-}
-
 template <bool KCF>
 __device__ __forceinline__ void rate_consts(const DevTab &t, int lr, int ty, double tt, double Rtti, int itt,
-                                            double dtt, double tbs, double &kf, double &kb, double lnT) {
+                                            double dtt, double tbs, double &kf, double &kb) {
   const int nr = t.nr;
   double A1 = ldg(t.arr_a + lr), B1 = ldg(t.arr_b + lr), E1 = ldg(t.arr_ea + lr);
   if (ty == 0 || ty == 1) {
-    kf = arrhenius(t, A1, B1, E1, tt, lnT, Rtti);
+    kf = A1;
+    if (B1 != 0.0) kf = kf * pow(tt, B1);
+    if (E1 != 0.0) kf = kf * exp(-E1 * Rtti);
   } else {
     double A2 = ldg(t.arr_a + nr + lr), B2 = ldg(t.arr_b + nr + lr), E2 = ldg(t.arr_ea + nr + lr);
-    double k0, kinf;
-    if (t.fused_arr) {
-      k0 = A1 * exp(B1 * lnT - E1 * Rtti);
-      kinf = A2 * exp(B2 * lnT - E2 * Rtti);
-    } else {
-      k0 = A1 * pow(tt, B1) * exp(-E1 * Rtti);
-      kinf = A2 * pow(tt, B2) * exp(-E2 * Rtti);
-    }
+    double k0 = A1 * pow(tt, B1) * exp(-E1 * Rtti);
+    double kinf = A2 * pow(tt, B2) * exp(-E2 * Rtti);
     double rpres = k0 * tbs / kinf;
     if (ty == 2) {
       kf = kinf * (rpres / (1.0 + rpres));
@@ -119,7 +101,6 @@ template <int NS, bool KCF = false>
 __device__ void chem_source(const DevTab &t, double tt, const double *conc, double *rhs, bool explicit_form) {
   const int nr = t.nr;
   double Rtti = 1.0 / (t.Ru * tt);
-  const double lnT = t.fused_arr ? log(tt) : 0.0;
   int itt;
   double dtt;
   kc_pos(t, tt, itt, dtt);
@@ -133,7 +114,7 @@ __device__ void chem_source(const DevTab &t, double tt, const double *conc, doub
       for (int k = 0; k < NS; k++) tbs = tbs + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k];
     }
     double kf, kb;
-    rate_consts<KCF>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb, lnT);
+    rate_consts<KCF>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb);
     double q1 = 1.0, q2 = 1.0;
 #pragma unroll
     for (int k = 0; k < NS; k++) {
@@ -165,7 +146,6 @@ template <int NS, int S>
 __device__ void chem_source_sp(const DevTab &t, double tt, const double *conc, double *rhs) {
   const int nr = t.nr;
   double Rtti = 1.0 / (t.Ru * tt);
-  const double lnT = t.fused_arr ? log(tt) : 0.0;
   int itt;
   double dtt;
   kc_pos(t, tt, itt, dtt);
@@ -179,7 +159,7 @@ __device__ void chem_source_sp(const DevTab &t, double tt, const double *conc, d
       for (int k = 0; k < NS; k++) tbs = tbs + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k * S];
     }
     double kf, kb;
-    rate_consts<false>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb, lnT);
+    rate_consts<false>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb);
     const int cnt = __ldg(t.sp_cnt + lr);
     const unsigned char *ix = t.sp_idx + (long long)lr * STX_SPW;
     const double *cf = t.sp_coef + (long long)lr * STX_SPW;

@@ -54,13 +54,7 @@ struct DevTab {
   int n_eoi;
   const double *aw_eoi, *coeff_eoi, *beta0;
   const int *nainsp;
-  // Arrhenius terms as A exp(b ln T - E/(R T)) (1, default) or A T^b exp(-E/(R T))
-  // (0, the reference's form; STX_ARRHENIUS=reference)
-  int fused_arr;
 };
-
-// the Arrhenius form a new context uses (STX_ARRHENIUS=reference: the reference's)
-int arrhenius_form_default();
 
 struct DevGrid {
   int nx, ny, nz, ng, nxg, nyg, nzg;

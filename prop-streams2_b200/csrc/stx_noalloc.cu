@@ -108,7 +108,6 @@ extern "C" int stx_rosenbrock_krylov_noalloc(const stx_params *par, const stx_ta
   DevPar &p = c.p;
   t = DevTab{};
   t.ns = tab->ns; t.nr = tab->nr; t.icl = tab->indx_cp_l; t.icr = tab->indx_cp_r; t.nset = tab->nsetcv;
-  t.fused_arr = arrhenius_form_default();
   t.ntab = tab->num_t_tab; t.ncp = t.icr - t.icl + 3; t.tmin = tab->t_min_tab; t.dtab = tab->dt_tab; t.Ru = tab->R_univ;
   t.mw = tab->mw; t.mwinv = tab->mwinv; t.rgas = tab->rgas; t.trange = tab->trange;
   t.cp = tab->cp_coeff; t.cv = tab->cv_coeff;

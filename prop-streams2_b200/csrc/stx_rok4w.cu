@@ -194,7 +194,6 @@ __device__ __noinline__ double cp_rhs_w(const DevCtx &c, double y, double T_iter
   __syncwarp();
   const int nr = t.nr;
   double Rtti = 1.0 / (t.Ru * tt);
-  const double lnT = t.fused_arr ? log(tt) : 0.0;
   int itt;
   double dtt;
   kc_pos(t, tt, itt, dtt);
@@ -207,7 +206,7 @@ __device__ __noinline__ double cp_rhs_w(const DevCtx &c, double y, double T_iter
       for (int k = 0; k < NS; k++) tbs = tbs + ldg(t.tb_eff + (long long)k * nr + lr) * conc[k];
     }
     double kf, kb;
-    rate_consts<false>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb, lnT);
+    rate_consts<false>(t, lr, ty, tt, Rtti, itt, dtt, tbs, kf, kb);
     const int cnt = __ldg(t.sp_cnt + lr);
     const unsigned char *ix = t.sp_idx + (long long)lr * STX_SPW;
     const double *cf = t.sp_coef + (long long)lr * STX_SPW;

@@ -46,9 +46,9 @@ import torch
 #    queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default), and work queued behind
 #    a long-running kernel in one stream then waits in every stream that shares
 #    its queue: 32 queues;
-#  * with lazy module loading (the default), the first launch of a kernel (or a
-#    stream capture that includes it) loads it and waits for the running
-#    kernels -- seconds behind a reactor launch: all kernels load at start.
+#  * with lazy module loading (the default) a kernel's module loads at its first
+#    launch or stream capture, in the middle of serving: all kernels load at
+#    start instead.
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 
@@ -86,11 +86,10 @@ class _GridJob:
 
 
 class _PinnedPool:
-    """Pinned host buffers in power-of-two size classes, kept for reuse.  A new
-    pinned allocation (cudaHostAlloc) can wait for the device to go idle, which
-    on a busy server means waiting for reactor launches that run for seconds;
-    served requests therefore stage their fields through buffers taken from
-    here, and allocations happen only while the pool warms up."""
+    """Pinned host buffers in power-of-two size classes, kept for reuse: served
+    requests stage their fields through buffers taken from here, so the loop
+    does not page-lock new host memory per request (flames of every size would
+    each need new buffers); allocations happen only while the pool warms up."""
 
     def __init__(self):
         self.free: Dict[int, List[torch.Tensor]] = {}
@@ -185,7 +184,7 @@ class Server:
     within the reactors the warp-per-reactor kernel runs at once on a B200, so
     every served batch, like a request served alone, takes that kernel)."""
 
-    def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 32, chunk: int = 5,
+    def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 8, chunk: int = 5,
                  reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 16,
                  graphs: bool = True):
         self.device = torch.device(device)
