@@ -12,10 +12,11 @@ compute_aux.
   python bench.py [--gpus N --steps K --warmup W]     # this implementation
   python bench.py --impl reference [...]              # the CPU reference arm
 
-Multi-GPU (torchrun, one rank per GPU): every rank advances its own 256^3 box
-(weak scaling); the CFL maxima are max-reduced over ranks each step, as the
-reference's mpi_allreduce does.  Ghost exchange between ranks is not part of
-this benchmark (each box is periodic on its own).
+Multi-GPU (torchrun, one rank per GPU): every rank advances a 256^3 z slab of
+a 256 x 256 x (256 N) periodic domain (weak scaling), exchanging its z ghost
+layers with the neighbouring ranks over NCCL at every swap of the step (the
+MPI half of the reference's bcswap); the CFL maxima are max-reduced over ranks
+each step, as the reference's mpi_allreduce does.
 """
 from __future__ import annotations
 
@@ -71,7 +72,8 @@ def config_dict(n, world, extra=None):
                      f"hybrid WENO5-Z/KEEP(2) + Ducros (threshold 0.1), mixture-averaged transport, "
                      f"Strang ROK4, Wray RK3, CFL 0.5",
          "cells_per_gpu": n ** 3, "species": 9, "reactions": 21, "precision_form": "plain FP64",
-         "parallelism": f"dp{world} (independent periodic boxes, global dt)",
+         "parallelism": (f"z-slab decomposition over {world} ranks of an {n}x{n}x{n * world} periodic domain, "
+                         f"NCCL ghost exchange at every swap, global dt") if world > 1 else "1 GPU, periodic box",
          "l2": "inputs larger than L2 (about 15 GB of fields per GPU)"}
     if extra:
         d.update(extra)
@@ -229,15 +231,23 @@ def run_stx(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     n = args.n
+    from stx import dist as D
+
     case = configs.turbulence_case(n)
-    W, WA = configs.turbulence_fields(case, args.seed + rank, xp=torch, device=dev)
+    # One rank: a periodic n^3 box.  Several: z slabs of an n x n x (n * world)
+    # periodic domain, the z ghosts exchanged with the neighbouring ranks over
+    # NCCL at every swap of the step (stx_set_exchange); every slab starts from
+    # the same seeded field, so the global field is the periodic continuation of
+    # one box and the interfaces carry no jump.
+    if world > 1:
+        D.make_z_slab(case)
+    W, WA = configs.turbulence_fields(case, args.seed, xp=torch, device=dev)
     sol = Solver(case, device=str(dev), w=W, w_aux=WA)
     del W, WA
+    exch = D.ZSlabExchange(sol).install() if world > 1 else None
     lib = sol.lib
     if args.precision == "mixed":
         sol.set_precision("mixed")
-
-    from stx import dist as D
 
     def compute_dt_global():
         out = (C.c_double * 9)()

@@ -127,6 +127,21 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
 int stx_ctx_create_like(const stx_ctx *base, const stx_params *par, const stx_grid *grid, stx_ctx **out);
 int stx_ctx_destroy(stx_ctx *ctx);
 
+/* Ghost exchange with neighbouring subdomains (the MPI half of the reference's
+ * bcswap, base_gpu.F90:1132-1264).  A face whose bctags entry is
+ * STX_BC_EXCHANGE is an interface: the library neither swaps it periodically
+ * nor applies a boundary condition to it.  After the local periodic swap of
+ * every stx_bcswap call (and so of every swap inside stx_rk_sync,
+ * stx_advance_solution and stx_update_ghost(do_swap = 1)) the library calls
+ * fn(user, stream, field, nvar) with the swapped fields (nvar consecutive
+ * ghosted fields) and the stream the call runs on; fn fills the interface
+ * ghosts (enqueued on that stream, or done) and returns 0, or an error that
+ * the library returns.  A context with an exchange cannot be captured
+ * (stx_graph_create returns STX_E_UNSUPPORTED).  fn = NULL removes it. */
+#define STX_BC_EXCHANGE (-1)
+typedef int (*stx_exchange_fn)(void *user, void *stream, double *field, int nvar);
+int stx_set_exchange(stx_ctx *ctx, stx_exchange_fn fn, void *user);
+
 /* eval_aux_cuf (kernels_gpu.F90:6154-6308): species clip written back into w,
  * primitives, Newton T(e), c, Bilger Z, Mathur lambda, Wilke mu, Bird rho*D_k,
  * over the 1-based box [istart,iend]x[jstart,jend]x[kstart,kend]. */

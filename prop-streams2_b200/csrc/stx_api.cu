@@ -21,6 +21,8 @@ struct stx_ctx {
   unsigned long long *dt_d;       // the nine CFL maxima
   double *time_d;                 // simulation time of captured steps (stx_graph_*)
   const DevCtx *dctx_d;           // device copy of d, for device functions that take the context by reference
+  stx_exchange_fn xfn = nullptr;   // ghost exchange at STX_BC_EXCHANGE faces (stx_set_exchange)
+  void *xuser = nullptr;
   WenoScratch weno;               // listed WENO faces of the staged sweeps (cap 0: none)
   int weno_list[3];               // per sweep direction: use the listed WENO faces
   std::vector<void *> allocs;
@@ -192,7 +194,7 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   if (par->nrk < 1 || par->nrk > 4) return STX_E_INVALID;
   for (int q = 0; q < 6; q++) {
     int t = par->bctags[q];
-    if (t != 0 && t != 1 && t != 2 && t != 8) return STX_E_UNSUPPORTED;
+    if (t != 0 && t != 1 && t != 2 && t != 8 && t != STX_BC_EXCHANGE) return STX_E_UNSUPPORTED;
     if (par->bctags_nr[q] != 0) return STX_E_UNSUPPORTED;
   }
   if (par->eul_imin != 1 || par->eul_imax != grid->nx || par->eul_jmin != 1 || par->eul_jmax != grid->ny ||
@@ -482,8 +484,22 @@ int stx_bcextr_var(stx_ctx *c, void *s, double *v) {
 
 int stx_bcswap(stx_ctx *c, void *s, double *f, int nvar) {
   if (!c || !f || nvar < 1) return STX_E_INVALID;
-  Prof pf(c, S(s), STX_K_GHOST, (c->periodic[0] || c->periodic[1] || c->periodic[2]) ? 1 : 0);
-  return launch_bcswap(c->d, S(s), f, nvar, c->periodic);
+  {
+    Prof pf(c, S(s), STX_K_GHOST, (c->periodic[0] || c->periodic[1] || c->periodic[2]) ? 1 : 0);
+    TRY(launch_bcswap(c->d, S(s), f, nvar, c->periodic));
+  }
+  if (c->xfn) {
+    int rc = c->xfn(c->xuser, s, f, nvar);
+    if (rc != 0) return rc < 0 ? rc : STX_E_INVALID;
+  }
+  return STX_OK;
+}
+
+int stx_set_exchange(stx_ctx *c, stx_exchange_fn fn, void *user) {
+  if (!c) return STX_E_INVALID;
+  c->xfn = fn;
+  c->xuser = fn ? user : nullptr;
+  return STX_OK;
 }
 
 int stx_update_ghost(stx_ctx *c, void *s, double *w, int do_swap) {
@@ -730,6 +746,7 @@ __global__ void k_time_set(double *t, double v) { *t = v; }
 int stx_graph_create(stx_ctx *c, const stx_fields *f, double dt, int nsteps, stx_graph **out) {
   if (!c || !f || !out || nsteps < 1 || !(dt > 0.0)) return STX_E_INVALID;
   *out = nullptr;
+  if (c->xfn) return STX_E_UNSUPPORTED;   // the exchange runs host code at every swap
   cudaStream_t cs;
   STX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   const int prof = c->prof_on;

@@ -400,17 +400,6 @@ int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, con
   }
 }
 
-// the thread-per-reactor kernel's shared-memory split (see launch_batch0d_setup)
-void batch0d_thread_carveout(int ns) {
-  switch (ns) {
-#define X(N) case N: cudaFuncSetAttribute(k_batch0d<N>, cudaFuncAttributePreferredSharedMemoryCarveout, \
-                                          (int)cudaSharedmemCarveoutMaxShared); break;
-    STX_FOR_NS(X)
-#undef X
-    default: break;
-  }
-}
-
 int launch_rosenbrock(const DevCtx &c, cudaStream_t s, double *w, double *wa, double dttry, double t0, double t1,
                       unsigned int *counter) {
   switch (c.t.ns) {

@@ -45,9 +45,8 @@ int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, con
                    double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
                    double *t_end, int *nsteps, unsigned int *counter);
 // once per device and species count: shared-memory split of the persistent
-// batched-reactor kernels (launch_batch0d_setup calls batch0d_thread_carveout)
+// warp-per-reactor kernel
 int launch_batch0d_setup(int ns);
-void batch0d_thread_carveout(int ns);
 // one warp per reactor (ns <= 32, nr <= 64, and unless force, no more reactors
 // than resident warps; STX_E_UNSUPPORTED otherwise)
 int launch_batch0d_warp(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,

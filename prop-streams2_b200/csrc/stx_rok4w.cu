@@ -337,13 +337,15 @@ static int batch0d_w_t(const DevCtx &c, cudaStream_t s, int n, const double *T0,
   }
 }
 
-// The batched-reactor kernels are persistent and can stay resident for seconds.
+// The warp-per-reactor kernel (the one small, served batches take) is persistent
+// and can stay resident for seconds.
 // An SM holding one of their CTAs keeps its shared-memory/L1 split until the CTA
 // exits, and a kernel that needs a larger shared-memory share (the staged
 // convective sweeps, ~90 KB per CTA) cannot start a CTA there meanwhile; on a
 // server that runs grid solves beside reactor launches those solves then wait
-// for the reactors.  So the reactor kernels ask for the largest shared-memory
-// split, which every other kernel fits beside.
+// for the reactors.  So the warp kernel asks for the largest shared-memory split,
+// which every other kernel fits beside.  (The thread-per-reactor kernel, for
+// large batches, keeps the default: its local working set needs the L1.)
 template <int NS>
 static void batch0d_carveout_t() {
   cudaFuncSetAttribute(k_batch0d_w<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -363,7 +365,6 @@ int launch_batch0d_setup(int ns) {
 #undef X
     default: break;
   }
-  batch0d_thread_carveout(ns);
   done.insert({dev, ns});
   return cudaGetLastError() == cudaSuccess ? STX_OK : STX_E_CUDA;
 }

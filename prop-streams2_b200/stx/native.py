@@ -82,12 +82,16 @@ _VP = C.c_void_p
 _I = C.c_int
 _D = C.c_double
 
+# stx_exchange_fn: int (*)(void *user, void *stream, double *field, int nvar)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int)
+
 # (name, restype, argtypes) of every entry point declared in include/stx.h
 STX_SIGNATURES = [
     ("stx_abi_version", C.c_int, []),
     ("stx_strerror", C.c_char_p, [_I]),
     ("stx_ctx_create", _I, [C.POINTER(StxParams), C.POINTER(StxTables), C.POINTER(StxGrid), C.POINTER(_VP)]),
     ("stx_ctx_create_like", _I, [_VP, C.POINTER(StxParams), C.POINTER(StxGrid), C.POINTER(_VP)]),
+    ("stx_set_exchange", _I, [_VP, EXCHANGE_FN, _VP]),
     ("stx_ctx_destroy", _I, [_VP]),
     ("stx_eval_aux", _I, [_VP, _VP, _VP, _VP, _I, _I, _I, _I, _I, _I]),
     ("stx_compute_aux", _I, [_VP, _VP, _VP, _VP, _I, _I]),
