@@ -184,7 +184,7 @@ class Server:
     within the reactors the warp-per-reactor kernel runs at once on a B200, so
     every served batch, like a request served alone, takes that kernel)."""
 
-    def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 8, chunk: int = 5,
+    def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 32, chunk: int = 5,
                  reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 16,
                  graphs: bool = True):
         self.device = torch.device(device)
