@@ -58,8 +58,8 @@ def parse():
     ap.add_argument("--graph-steps", type=int, default=10, help="steps per captured graph (--workload flame)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="fp64: the reference method; mixed: FP32 face fluxes and transport, FP64 residual/chemistry")
-    ap.add_argument("--requests", type=int, default=1000, help="requests of the served mix (--workload serve)")
-    ap.add_argument("--rate", type=float, default=20.0, help="Poisson arrival rate [1/s] (--workload serve)")
+    ap.add_argument("--requests", type=int, default=600, help="requests of the served mix (--workload serve)")
+    ap.add_argument("--rate", type=float, default=10.0, help="Poisson arrival rate [1/s] (--workload serve)")
     ap.add_argument("--reactors", type=int, default=8192, help="reactors per GPU (--workload reactors)")
     ap.add_argument("--t-max", type=float, default=1e-2, help="longest integration of a reactor [s]")
     ap.add_argument("--max-steps", type=int, default=20000, help="ROK4 step cap per reactor")
