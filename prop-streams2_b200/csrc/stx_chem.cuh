@@ -15,6 +15,11 @@
 #endif
 
 
+// x^e for a stoichiometric exponent: the square as one product (the reference's
+// x**2.0 through pow costs a logarithm and an exponential), any other
+// exponent through pow.
+__device__ __forceinline__ double stoich_pow(double x, double e) { return e == 2.0 ? x * x : pow(x, e); }
+
 // Temperature-table position of T for K_c (kernels_gpu.F90:9259-9264).
 __device__ __forceinline__ void kc_pos(const DevTab &t, double tt, int &itt, double &dtt) {
   itt = (int)((tt - t.tmin) / t.dtab) + 1;
@@ -59,7 +64,8 @@ __device__ __forceinline__ void rate_consts(const DevTab &t, int lr, int ty, dou
         double noff = 0.75 - 1.27 * fcent;
         double doff = 0.14;
         double lp = log10(rpres);
-        double foff = pow(10.0, pow(1.0 + pow((lp + coff) / (noff - doff * (lp + coff)), 2.0), -1.0) * fcent);
+        const double tr = (lp + coff) / (noff - doff * (lp + coff));
+        double foff = pow(10.0, (1.0 / (1.0 + tr * tr)) * fcent);   // (1 + tr^2)^-1 as a product and a division
         kf = kinf * (rpres / (1.0 + rpres)) * foff;
       }
     } else if (ty == 4) {
@@ -120,9 +126,9 @@ __device__ void chem_source(const DevTab &t, double tt, const double *conc, doub
     for (int k = 0; k < NS; k++) {
       double rr = ldg(t.r_coeffs + (long long)k * nr + lr), pp = ldg(t.p_coeffs + (long long)k * nr + lr);
       if (rr == 1.0) q1 = q1 * conc[k];
-      else if (rr != 0.0) q1 = q1 * pow(conc[k], rr);
+      else if (rr != 0.0) q1 = q1 * stoich_pow(conc[k], rr);
       if (pp == 1.0) q2 = q2 * conc[k];
-      else if (pp != 0.0) q2 = q2 * pow(conc[k], pp);
+      else if (pp != 0.0) q2 = q2 * stoich_pow(conc[k], pp);
     }
     double tb = (ty == 1) ? tbs : 1.0;
     double qlr = tb * (kf * q1 - kb * q2);
@@ -168,13 +174,13 @@ __device__ void chem_source_sp(const DevTab &t, double tt, const double *conc, d
     for (int n = 0; n < (cnt & 255); n++) {
       double x = conc[__ldg(ix + n) * S], e = ldg(cf + n);
       if (e == 1.0) q1 = q1 * x;
-      else q1 = q1 * pow(x, e);
+      else q1 = q1 * stoich_pow(x, e);
     }
 #pragma unroll 1
     for (int n = 0; n < ((cnt >> 8) & 255); n++) {
       double x = conc[__ldg(ix + STX_SPR + n) * S], e = ldg(cf + STX_SPR + n);
       if (e == 1.0) q2 = q2 * x;
-      else q2 = q2 * pow(x, e);
+      else q2 = q2 * stoich_pow(x, e);
     }
     double tb = (ty == 1) ? tbs : 1.0;
     double qlr = tb * (kf * q1 - kb * q2);

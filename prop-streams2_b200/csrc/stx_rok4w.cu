@@ -215,13 +215,13 @@ __device__ __noinline__ double cp_rhs_w(const DevCtx &c, double y, double T_iter
     for (int n = 0; n < (cnt & 255); n++) {
       double x = conc[__ldg(ix + n)], e = ldg(cf + n);
       if (e == 1.0) q1 = q1 * x;
-      else q1 = q1 * pow(x, e);
+      else q1 = q1 * stoich_pow(x, e);
     }
 #pragma unroll 1
     for (int n = 0; n < ((cnt >> 8) & 255); n++) {
       double x = conc[__ldg(ix + STX_SPR + n)], e = ldg(cf + STX_SPR + n);
       if (e == 1.0) q2 = q2 * x;
-      else q2 = q2 * pow(x, e);
+      else q2 = q2 * stoich_pow(x, e);
     }
     double tb = (ty == 1) ? tbs : 1.0;
     qr[lr] = tb * (kf * q1 - kb * q2);
