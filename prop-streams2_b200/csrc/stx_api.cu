@@ -413,7 +413,12 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
     const unsigned int *wc = nullptr;
     const int *wl = nullptr;
     const double *wf = nullptr;
-    if (cap < 0x7fffffffLL) {
+    // the scratch is an optimisation: a grid whose face buffers would take more
+    // than a quarter of the free device memory runs without it (WENO in line)
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const double need = (double)cap * (sizeof(int) + sizeof(double) * c->nv);
+    if (cap < 0x7fffffffLL && need <= 0.25 * (double)free_b) {
       if ((rc = upload<unsigned int>(c, nullptr, 1, &wc))) return fail(rc);
       if ((rc = upload<int>(c, (const int *)nullptr, (size_t)cap, &wl))) return fail(rc);
       if ((rc = upload<double>(c, nullptr, (size_t)cap * c->nv, &wf))) return fail(rc);
