@@ -655,7 +655,9 @@ def stiff_config(n, world):
             "parallelism": f"dp{world} (independent boxes)",
             "size_note": f"{n}^3 stands in for the 128^3 case: at dt 1e-10 s every cell takes thousands of "
                          "adaptive sub-steps, each with 57 right-hand sides of 325 reactions, so a 128^3 step "
-                         "runs for minutes; the per-cell work does not depend on the box size",
+                         "runs for hours; the per-cell work does not depend on the box size, but "
+                         f"{n ** 3} cells (one thread each) occupy a small part of the GPU, so this rate "
+                         "understates what a full box sustains",
             "l2": "compute bound (per-cell Jacobian)"}
 
 

@@ -8,6 +8,11 @@
 // face flux -- and the species enthalpies of the shared point -- in registers.
 #include "stx_kernels.cuh"
 
+// CTAs per SM the viscous sweeps' register budget is sized for
+#ifndef STX_VISC_MINB
+#define STX_VISC_MINB 1
+#endif
+
 // One staggered face between points p (left) and q = p + st (right), computed in
 // R (double: plain form; float: mixed form, fields rounded once on load).  hl
 // carries the species enthalpies at
@@ -79,7 +84,7 @@ __device__ __forceinline__ void visc_face(const DevCtx &c, const double *__restr
 // threads whose face is not the first of its row form the divergence -- every
 // thread busy for any nx.
 template <int NS, typename R>
-__global__ void __launch_bounds__(128) k_visc_x(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl) {
+__global__ void __launch_bounds__(128, STX_VISC_MINB) k_visc_x(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
   constexpr int XB = xsweep_block(NS);
@@ -111,7 +116,7 @@ __global__ void __launch_bounds__(128) k_visc_x(DevCtx c, const double *__restri
 }
 
 template <int NS, int DIR, typename R>
-__global__ void __launch_bounds__(128) k_visc_yz(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl, int chunk) {
+__global__ void __launch_bounds__(128, STX_VISC_MINB) k_visc_yz(DevCtx c, const double *__restrict__ wa, double *__restrict__ fl, int chunk) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
