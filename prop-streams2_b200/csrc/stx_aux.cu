@@ -6,6 +6,14 @@
 // once with unit-stride (i-fastest) coalesced accesses.
 #include "stx_kernels.cuh"
 
+// CTAs per SM the eval_aux register budget is sized for: 8 (64 registers, some
+// spilled) ran compute_aux on a developed 128^3 field in 1.09 ms against 1.48 ms
+// unconstrained (154 registers), 1.22 ms at 4 and 1.14 ms at 6, with the same
+// results bit for bit
+#ifndef STX_AUX_MINB
+#define STX_AUX_MINB 8
+#endif
+
 // ============================================================== eval_aux
 // eval_aux_cuf (kernels_gpu.F90:6154-6308).  Differences in arithmetic order
 // from the reference: the Wilke factor sqrt(mu_m/mu_l) is formed as
@@ -13,7 +21,7 @@
 // (W_m/W_l)^0.25 come from a host table; both change results only at rounding
 // level.  The species clip is stored only where it changes w.
 template <int NS, typename R>
-__global__ void __launch_bounds__(128) k_eval_aux(DevCtx c, double *__restrict__ w, double *__restrict__ wa,
+__global__ void __launch_bounds__(128, STX_AUX_MINB) k_eval_aux(DevCtx c, double *__restrict__ w, double *__restrict__ wa,
                                                   int i0, int j0, int k0, int ni, int nj, int nk) {
   const DevGrid &g = c.g;
   const DevTab &t = c.t;

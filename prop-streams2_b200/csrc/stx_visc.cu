@@ -8,9 +8,12 @@
 // face flux -- and the species enthalpies of the shared point -- in registers.
 #include "stx_kernels.cuh"
 
-// CTAs per SM the viscous sweeps' register budget is sized for
+// CTAs per SM the viscous sweeps' register budget is sized for: 4 (128
+// registers, a few spilled) ran the three sweeps 1.45x faster on a developed
+// 128^3 field than the unconstrained 164 registers (3 CTAs per SM), whose
+// loads were latency-bound at 12 warps per SM
 #ifndef STX_VISC_MINB
-#define STX_VISC_MINB 1
+#define STX_VISC_MINB 4
 #endif
 
 // One staggered face between points p (left) and q = p + st (right), computed in
