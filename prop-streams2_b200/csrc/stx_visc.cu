@@ -8,12 +8,15 @@
 // face flux -- and the species enthalpies of the shared point -- in registers.
 #include "stx_kernels.cuh"
 
-// CTAs per SM the viscous sweeps' register budget is sized for: 4 (128
-// registers, a few spilled) ran the three sweeps 1.45x faster on a developed
-// 128^3 field than the unconstrained 164 registers (3 CTAs per SM), whose
-// loads were latency-bound at 12 warps per SM
+// CTAs per SM the viscous sweeps' register budget is sized for.  Unconstrained
+// they take 164 registers (3 CTAs per SM), and their loads are latency-bound at
+// 12 warps per SM.  On a developed 128^3 field, mode 1: 5 CTAs per SM (102
+// registers, some spilled) ran a call in 2.06 ms, 4 in 2.41 ms, 6 in 2.13 ms,
+// and the unconstrained kernel about 1.45x slower than 4, with the same results
+// bit for bit.  With 53 species (spilled at any budget) a 48^3 call took
+// 3.41-3.50 ms unconstrained, at 4 and at 5
 #ifndef STX_VISC_MINB
-#define STX_VISC_MINB 4
+#define STX_VISC_MINB 5
 #endif
 
 // One staggered face between points p (left) and q = p + st (right), computed in
