@@ -654,6 +654,14 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const DevC
 //  5. every cell forms fl += (fhat_f - fhat_{f-1}) dxi/dx from the staged faces.
 // It covers ep_order <= 6 and weno_scheme <= 3 (the 3-cell halo) and ns <= 20
 // (shared memory); euler_r dispatches to the per-face sweeps otherwise.
+// CTAs per SM the x tile's register budget is sized for: 5 (96 registers; its
+// 39 KB of shared memory also admits 5) ran an x sweep of a developed 128^3
+// field in 0.585 ms against 0.679 ms at 4 (128 registers), with the same
+// results bit for bit.  y and z: 2, where their 91 KB of shared memory also
+// sets the limit
+#ifndef STX_ETILE_X_MINB
+#define STX_ETILE_X_MINB 5
+#endif
 template <int NS, int DIR> struct ETile {
   static constexpr int TC = DIR == 0 ? 64 : 16;        // cells per line updated by a CTA
   static constexpr int NL = DIR == 0 ? 2 : 16;         // lines per CTA
@@ -699,7 +707,7 @@ __device__ __forceinline__ int etile_field(int v) {
 }
 
 template <int NS, int DIR, typename R>
-__global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? 4 : 2)
+__global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MINB : 2)
     k_euler_tile(DevCtx c, const DevCtx *__restrict__ cg, const double *__restrict__ wa, double *__restrict__ fl,
                  int nmin, int nmax, int overwrite, const double *__restrict__ fhw, long long cap) {
   using T = ETile<NS, DIR>;
