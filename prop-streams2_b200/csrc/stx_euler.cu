@@ -987,8 +987,15 @@ __global__ void __launch_bounds__(256) k_weno_mark(DevCtx c, const double *__res
   }
 }
 
+// CTAs per SM the listed-WENO pass's register budget is sized for: 4 (128
+// registers) ran a y sweep of a developed 128^3 field (mark, list and tile) in
+// 0.921 ms, 6 (80 registers) in 0.939 ms and 8 (64) in 0.945 ms, with the same
+// results bit for bit
+#ifndef STX_WLIST_MINB
+#define STX_WLIST_MINB 4
+#endif
 template <int NS, int DIR>
-__global__ void __launch_bounds__(128, 4) k_weno_list(DevCtx c, const DevCtx *__restrict__ cg,
+__global__ void __launch_bounds__(128, STX_WLIST_MINB) k_weno_list(DevCtx c, const DevCtx *__restrict__ cg,
                                                       const double *__restrict__ wa, int nmin, int nmax,
                                                       const unsigned int *__restrict__ count,
                                                       const int *__restrict__ list, double *__restrict__ fh,
