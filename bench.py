@@ -63,7 +63,46 @@ def parse():
     ap.add_argument("--reactors", type=int, default=8192, help="reactors per GPU (--workload reactors)")
     ap.add_argument("--t-max", type=float, default=1e-2, help="longest integration of a reactor [s]")
     ap.add_argument("--max-steps", type=int, default=20000, help="ROK4 step cap per reactor")
+    ap.add_argument("--ncu-raw", default=None,
+                    help="an ncu --page raw --csv export of the dominant kernel class's launch(es) captured on this "
+                         "box; its dram__bytes_read.sum + dram__bytes_write.sum per launch, scaled by cells to this "
+                         "workload's launch, becomes roofline.traffic (null without it)")
+    ap.add_argument("--ncu-cells", type=int, default=0, help="interior cells of the --ncu-raw capture's case")
     return ap.parse_args()
+
+
+# kernel-name prefixes of the HBM-class kernel classes (for --ncu-raw)
+KERNELS_OF_CLASS = {"euler": ("k_euler", "k_weno"), "visc": ("k_visc",), "eval_aux": ("k_eval_aux",),
+                    "rk": ("k_update_field", "k_init_flux")}
+
+
+def ncu_traffic(path, prefixes, cells_captured, cells_here):
+    """DRAM bytes per launch of a kernel class from an ncu raw CSV export
+    (ncu -i <rep> --page raw --csv): the mean over the captured launches of
+    dram__bytes_read.sum + dram__bytes_write.sum, summed over the class's
+    kernels, scaled by cells to this workload (traffic grows with the cells
+    processed).  None without a capture."""
+    if not path or not prefixes or cells_captured <= 0:
+        return None
+    import csv
+    with open(path) as fh:
+        rows = list(csv.reader(fh))
+    head = rows[0]
+    ik = head.index("Kernel Name")
+    ir, iw = head.index("dram__bytes_read.sum"), head.index("dram__bytes_write.sum")
+    units = rows[1]
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    per_kernel = {}
+    for r in rows[2:]:
+        if not any(r[ik].startswith(p) for p in prefixes):
+            continue
+        b = float(r[ir].replace(",", "")) * scale.get(units[ir], 1.0) + \
+            float(r[iw].replace(",", "")) * scale.get(units[iw], 1.0)
+        per_kernel.setdefault(r[ik].split("(")[0].split("<")[0], []).append(b)
+    if not per_kernel:
+        return None
+    total = sum(sum(v) / len(v) for v in per_kernel.values())
+    return total * cells_here / cells_captured
 
 
 def config_dict(n, world, extra=None):
@@ -331,8 +370,8 @@ def run_stx(args):
     wbytes = sol.w.numel() * 8
 
     # ---------------- roofline of the dominant HBM-bound kernel class
-    cls = {KNAMES[k]: {"launches": int(prof[k].launches), "ms": prof[k].ms, "bytes": prof[k].bytes}
-           for k in range(8)}
+    cls = {KNAMES[k]: {"launches": int(prof[k].launches), "calls": int(prof[k].timed), "ms": prof[k].ms,
+                       "bytes": prof[k].bytes} for k in range(8)}
     tot_ms = sum(v["ms"] for v in cls.values()) or 1.0
     for v in cls.values():
         v["share"] = v["ms"] / tot_ms
@@ -345,18 +384,16 @@ def run_stx(args):
         with open(peaks_fn) as fh:
             peak = float(json.load(fh)["hbm_gbs"])
         peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
-    # DRAM bytes per algorithmic byte of the kernel class, from one ncu capture
-    # at 96^3 (profiles/k_visc_yz_turbulence96_h2air9.md: 363.3 of 354.0 MB;
-    # profiles/k_euler_tile_turbulence96_h2air9.md: 325.7 of 304.3 MB); the
-    # traffic grows in proportion to the cells, so it scales to this launch
-    dram_per_alg = {"visc": 363.3 / 354.0, "euler": 325.7 / 304.3}
-    bpl = cls[dom]["bytes"] / max(1, cls[dom]["launches"])
-    traffic = dram_per_alg[dom] * bpl if dom in dram_per_alg else None
+    # one "launch" of a class is one entry-point call: a fused sweep may run up
+    # to three kernels (listed WENO faces: mark, list, staged tile)
+    traffic = ncu_traffic(args.ncu_raw, KERNELS_OF_CLASS.get(dom, ()), args.ncu_cells, n ** 3)
     ach = cls[dom]["gbs"]
     roofline = {"bound": "hbm", "kernel_class": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak if ach else None, "traffic": traffic, "peak_source": peak_src,
-                "launches": cls[dom]["launches"],
-                "bytes_per_launch": cls[dom]["bytes"] / max(1, cls[dom]["launches"])}
+                "calls": cls[dom]["calls"], "kernel_launches": cls[dom]["launches"],
+                "bytes_per_launch": cls[dom]["bytes"] / max(1, cls[dom]["calls"]),
+                "traffic_source": ("ncu capture " + os.path.basename(args.ncu_raw)) if traffic else
+                "null: no ncu capture given (--ncu-raw)"}
 
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -527,10 +564,10 @@ FLAME_PUBLISHED = 2000.0 / 7.0269314e-3
 
 
 def flame_config(world, graph_steps):
-    return {"workload": "1-D laminar premixed H2/air flame, 2000 cells over 0.03 m, 11 species / 21 reactions "
-                        "(examples/laminar_premix_flame settings: inflow xmin, extrapolation xmax, WENO5-Z on every "
-                        "face + KEEP(2), simpler splitting, ROK4, Wray RK3, fixed dt 1e-8 s); synthetic tanh flame "
-                        "(phi 0.6, 298 K -> 1847 K) standing in for premix.dat",
+    return {"workload": "1-D laminar premixed H2/air flame, 2000 cells over 0.03 m, 11 species / 21 reactions: "
+                        "examples/laminar_premix_flame as the reference runs it (its multideal.ini: inflow xmin, "
+                        "extrapolation xmax, WENO5-Z on every face + KEEP(2), simpler splitting, ROK4, Wray RK3, "
+                        "fixed dt 1e-8 s; its premix.dat initial profile)",
             "cells_per_gpu": 2000, "species": 11, "reactions": 21, "precision_form": "plain FP64",
             "parallelism": f"dp{world} (independent flames)",
             "launch": f"{graph_steps} steps per CUDA graph launch",
@@ -547,7 +584,7 @@ def cpu_flame(args, budget_s=20.0):
     from stx import configs
     from driver import OracleSolver
     cores = os.cpu_count() or 1
-    o = OracleSolver(configs.flame_case(2000, phi=0.6, Tu=298.0), threads=cores)
+    o = OracleSolver(configs.premix_flame_case(), threads=cores)
     o.prepare()
     o.step()
     t0 = time.perf_counter()
@@ -575,7 +612,7 @@ def run_flame(args):
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-    case = configs.flame_case(2000, phi=0.6, Tu=298.0)
+    case = configs.premix_flame_case()
     sol = Solver(case, device=str(dev))
     sol.prepare()
     G = max(1, args.graph_steps)
@@ -626,7 +663,8 @@ def run_flame(args):
     wbytes = sol.w.numel() * 8
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": args.warmup,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": value / (FLAME_PUBLISHED * world), "dtype": "f64", "data": "synthetic (seeded)",
+            "vs_baseline": value / (FLAME_PUBLISHED * world), "dtype": "f64",
+            "data": "the reference's own input (examples/laminar_premix_flame/premix.dat)",
             "config": flame_config(world, G), "clocks": ck, "gpu_launches": K // G,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": wbytes, "d2h_bytes_per_step": wbytes,
                     "path": "Solver.step (stx_compute_aux / stx_advance_solution through the C ABI, ~50 launches "

@@ -43,6 +43,7 @@ extern "C" {
 #define STX_E_NOMEM      -3   /* device allocation failed (stx_ctx_create only) */
 #define STX_E_UNSUPPORTED -4  /* option outside the supported hot path (e.g. IBM, LES, NR BCs) */
 #define STX_E_TOO_LARGE  -5   /* problem larger than the fixed scratch of stx_rosenbrock_krylov_noalloc */
+#define STX_E_LOCAL_MEM  -6   /* stx_rosenbrock_krylov_noalloc: cudaLimitStackSize below the kernel's local frame */
 
 /* status bits accumulated on the device (stx_status) */
 #define STX_ST_NEWTON_CAP     0x1u  /* a Newton T(e) inversion hit its 10-iteration cap */
@@ -88,8 +89,13 @@ typedef struct stx_params {
   int32_t ep_order, nkeep, weno_scheme, weno_version, flux_splitting;
   int32_t sensor_type, visc_order, conservative_viscous;
   double  sensor_threshold;
-  int32_t bctags[6];                           /* xmin,xmax,ymin,ymax,zmin,zmax; 0 = periodic */
-  int32_t bctags_nr[6];                        /* must be 0 (non-reflecting BCs not on this path) */
+  int32_t bctags[6];                           /* xmin,xmax,ymin,ymax,zmin,zmax: 0 periodic, 1 free stream
+                                                  (xmin), 2 extrapolation, 4 subsonic extrapolation at p0,
+                                                  5 symmetry (y), 6 isothermal wall (y), 7 open outflow,
+                                                  8 adiabatic wall */
+  int32_t bctags_nr[6];                        /* characteristic treatment of the face (bc_nr): 0 none,
+                                                  1 non-reflecting, 2 relaxed to the outer ghost, 3 relaxed
+                                                  to winf, 6 reflecting wall */
   int32_t force_zero_flux[6];
   int32_t eul_imin, eul_imax, eul_jmin, eul_jmax, eul_kmin, eul_kmax;
   int32_t enable_chemistry;                    /* 0 off, 1 explicit source, 2 implicit Rosenbrock */
@@ -100,6 +106,7 @@ typedef struct stx_params {
   int32_t nrk;                                 /* 3: Wray RK3 */
   double  rhork[4], gamrk[4];
   const double *winf;                          /* (nv) free-stream state for bc tag 1, may be NULL */
+  double  T_wall;                              /* wall temperature of bc tag 6 ([flow] T_wall) */
 } stx_params;
 
 /* Field set of one solve (all device pointers). */
@@ -156,8 +163,18 @@ int stx_bcextr_var(stx_ctx *ctx, void *stream, double *var);
 /* base_gpu%bcswap / bcswap_var (base_gpu.F90:1132-1264) on one GPU: periodic
  * self-exchange of the ng ghost layers of nvar consecutive ghosted fields. */
 int stx_bcswap(stx_ctx *ctx, void *stream, double *field, int nvar);
-/* update_ghost (multideal_gpu.F90:1165-1238) for bc tags 0,1,2,8; do_swap as in the reference. */
+/* update_ghost (multideal_gpu.F90:1165-1238): the ghost fills of every face's bc
+ * tag, then, with do_swap = 1, the periodic swap (as in the reference).  Tags 4
+ * (bcextr_sub_cuf) and 6 (bcwall_cuf) read and write w_aux (the mass fractions
+ * of the cells they use, the Newton guess of tag 6): stx_update_ghost_aux takes
+ * it; stx_update_ghost returns STX_E_INVALID for them. */
 int stx_update_ghost(stx_ctx *ctx, void *stream, double *w, int do_swap);
+int stx_update_ghost_aux(stx_ctx *ctx, void *stream, double *w, double *w_aux, int do_swap);
+/* bc_nr (multideal_gpu.F90:1116-1163, kernels_gpu.F90:4330-4793): the
+ * characteristic treatment of the boundary cells of every face with
+ * bctags_nr > 0, added to fl (the faces' cells are outside the eul_* range of
+ * the convective sweeps).  stx_rk_sync calls it after the viscous fluxes. */
+int stx_bc_nr(stx_ctx *ctx, void *stream, const double *w_aux, const double *w, double *fl);
 
 /* euler_x/y/z (multideal_gpu.F90:877-1044): hybrid central-KEEP / WENO face
  * fluxes (kernels_gpu.F90:88-2063) fused with the divergence update
@@ -186,6 +203,15 @@ int stx_rk_finish(stx_ctx *ctx, void *stream, double *w, const double *fl, doubl
 /* compute_dt_cuf (kernels_gpu.F90:6075-6152): the nine CFL maxima.  Writes
  * out9 (host memory) after synchronising the stream. */
 int stx_compute_dt(stx_ctx *ctx, void *stream, const double *w_aux, const int32_t *fluid_mask, double out9[9]);
+
+/* compute_residual (multideal_gpu.F90:1585-1615, kernels_gpu.F90:5991-6011,
+ * 6038-6073) on one process: out7 = {residual_rhou = sqrt(sum over fluid
+ * interior cells of (fln(I_U)/dt)^2 / (nx ny nz)), rhomin, rhomax, tmin, tmax,
+ * pmin, pmax}, the figures print_progress writes every print_control steps.
+ * The sum is formed in a fixed order (the same result on every call).  Writes
+ * out7 (host memory) after synchronising the stream. */
+int stx_compute_residual(stx_ctx *ctx, void *stream, const double *fln, const double *w_aux,
+                         const int32_t *fluid_mask, double dt, double out7[7]);
 
 /* Chemistry.  rosenbrock (multideal_gpu.F90:694-753 -> kernels_gpu.F90:8928-9501),
  * rosenbrock_krylov (:755-837 -> :10360-11205), compute_chemistry (:9503-9674). */
@@ -251,9 +277,22 @@ int stx_batch0d_integrate(stx_ctx *ctx, void *stream, int n, const double *T0, c
  * Its scratch is a 4-byte file-scope device array (the work-stealing cell
  * counter) loaded with the library on each device and kept until the process
  * exits; it allocates nothing.  At most 2^31 cells per call (STX_E_TOO_LARGE
- * beyond).  The first call on a device looks up the scratch's device address,
- * so make it before any stream capture.  Calls share the scratch: each call
- * clears it first, and calls that overlap on the GPU race on it. */
+ * beyond).  Calls share the scratch: each call clears it first, and calls that
+ * overlap on the GPU race on it.
+ * Set-up: the first call on a device loads the kernel (the CUDA runtime's module
+ * load, once per device) and looks up the scratch's device address, so make it
+ * before any stream capture.  The address stays valid for the life of the
+ * device's primary context: do not call again on a device after resetting it
+ * (cudaDeviceReset).  stream must belong to the current device (STX_E_INVALID
+ * otherwise).
+ * Local memory: the kernel's per-thread working set lives in local memory,
+ * which the driver backs with cudaLimitStackSize bytes for every thread the
+ * device can hold, and grows by a device allocation when a launch needs more.
+ * So that no call allocates, a call whose kernel needs more than the current
+ * limit launches nothing and returns STX_E_LOCAL_MEM.  Raise the limit once at
+ * initialisation, e.g. cudaDeviceSetLimit(cudaLimitStackSize, 4608) for up to
+ * 14 species or 12288 for 53 (this build's frames: 3168 B at 9 species, 3904 B
+ * at 14, 10528 B at 53; the call checks the kernel's actual figure). */
 int stx_rosenbrock_krylov_noalloc(const stx_params *par, const stx_tables *tab_dev, const stx_grid *grid,
                                   void *stream, double *w, const double *w_aux, const double *fl_sav,
                                   double dttry, double time_start, double time_end, int simpler, uint32_t *status);

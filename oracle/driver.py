@@ -58,7 +58,7 @@ class OracleSolver:
 
     # thin wrappers with the reference's names
     def update_ghost(self, do_swap=1):
-        self.lib.ox_update_ghost(self.ctx, _ptr(self.w), do_swap)
+        self.lib.ox_update_ghost_aux(self.ctx, _ptr(self.w), _ptr(self.w_aux), do_swap)
 
     def compute_aux(self, central=1, ghost=1):
         self.lib.ox_compute_aux(self.ctx, _ptr(self.w), _ptr(self.w_aux), central, ghost)

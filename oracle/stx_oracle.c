@@ -236,6 +236,33 @@ static double species_poly_int(const ox_ctx *c, const double *arr, double tt, in
   return hh;
 }
 
+/* get_mixture_e_from_temperature_dev (kernels_gpu.F90:7047-7102): the mixture's
+ * internal energy at tt with the mass fractions in w_aux(p, 1..ns) */
+static double mixture_e_wa(const ox_ctx *c, double tt, const double *wa, size_t p) {
+  int nrange[MAXNS];
+  for (int lsp = 1; lsp <= NS; lsp++) nrange[lsp - 1] = c->t.nsetcv > 1 ? locate_range(c, tt, lsp) : 1;
+  double ee = 0.0;
+  for (int lsp = 1; lsp <= NS; lsp++) ee = ee + CPC(c->cv, c->t.indx_cp_r + 1, lsp, nrange[lsp - 1]) * WG(wa, p, lsp);
+  for (int l = c->t.indx_cp_l; l <= c->t.indx_cp_r; l++) {
+    double tprod = l == -1 ? log(tt) : ipow(tt, l + 1) / (l + 1.0);
+    double cv_l = 0.0;
+    for (int lsp = 1; lsp <= NS; lsp++) cv_l = cv_l + CPC(c->cv, l, lsp, nrange[lsp - 1]) * WG(wa, p, lsp);
+    ee = ee + cv_l * tprod;
+  }
+  return ee;
+}
+/* get_rho_from_w_dev (:6902-6915) and get_rmixture (:6917-6931) */
+static double rho_from_w(const ox_ctx *c, const double *w, size_t p) {
+  double rho = WG(w, p, 1);
+  for (int lsp = 2; lsp <= NS; lsp++) rho = rho + WG(w, p, lsp);
+  return rho;
+}
+static double rmix_wa(const ox_ctx *c, const double *wa, size_t p) {
+  double rm = c->rgas[0] * WG(wa, p, 1);
+  for (int lsp = 2; lsp <= NS; lsp++) rm = rm + c->rgas[lsp - 1] * WG(wa, p, lsp);
+  return rm;
+}
+
 /* ---------------------------------------------------------------- eval_aux */
 /* eval_aux_cuf body (kernels_gpu.F90:6188-6302) for one point */
 static void aux_point(ox_ctx *c, double *w, double *wa, size_t p) {
@@ -455,12 +482,134 @@ void ox_bcswap(ox_ctx *c, double *f, int nvar) {
   free(b1); free(b2); free(b3); free(b4); free(b5); free(b6);
 }
 
+/* the ghost point l of face ilat (1..6) at tangential indices (a, b), and the
+ * interior point at normal index n (1..nx etc.) on the same line */
+static size_t face_pt(const ox_ctx *c, int ilat, int a, int b, int n) {
+  int dir = (ilat - 1) / 2;
+  if (dir == 0) return gi(c, n, a, b);
+  if (dir == 1) return gi(c, a, n, b);
+  return gi(c, a, b, n);
+}
+
+/* bcextr_sub_cuf (kernels_gpu.F90:4092-4327), every side: the boundary cell's
+ * mass fractions into w_aux, then ng ghosts with its species and momentum and the
+ * energy of T = p0 / (rho R_mix) */
+static void bc_extr_sub(ox_ctx *c, int ilat, double *w, double *wa) {
+  int dir = (ilat - 1) / 2, hi = (ilat - 1) % 2, ng = c->g.ng;
+  int n = dir == 0 ? c->g.nx : (dir == 1 ? c->g.ny : c->g.nz);
+  int na = dir == 0 ? c->g.ny : c->g.nx, nb = dir == 2 ? c->g.ny : c->g.nz;
+  int ib = hi ? n : 1;
+  for (int b = 1; b <= nb; b++)
+    for (int a = 1; a <= na; a++) {
+      size_t p = face_pt(c, ilat, a, b, ib);
+      double rho = rho_from_w(c, w, p);
+      for (int lsp = 1; lsp <= NS; lsp++) WG(wa, p, lsp) = WG(w, p, lsp) / rho;
+    }
+  for (int b = 1; b <= nb; b++)
+    for (int a = 1; a <= na; a++)
+      for (int l = 1; l <= ng; l++) {
+        size_t p = face_pt(c, ilat, a, b, ib), q = face_pt(c, ilat, a, b, hi ? n + l : 1 - l);
+        double rho = rho_from_w(c, w, p);
+        double rhou = WG(w, p, I_U), rhov = WG(w, p, I_V), rhow = WG(w, p, I_W);
+        double rmixtloc = rmix_wa(c, wa, p);
+        double tt = c->p.p0 / rho / rmixtloc;
+        double ee = mixture_e_wa(c, tt, wa, p);
+        for (int lsp = 1; lsp <= NS; lsp++) WG(w, q, lsp) = WG(w, p, lsp);
+        WG(w, q, I_U) = rhou;
+        WG(w, q, I_V) = rhov;
+        WG(w, q, I_W) = rhow;
+        WG(w, q, I_E) = rho * ee + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
+      }
+}
+
+/* bcwall_cuf (kernels_gpu.F90:5437-5545): isothermal wall on the y sides (the
+ * x and z sides do nothing): the first ng interior layers' mass fractions into
+ * w_aux, then ghost 1-l (ny+l) mirrors layer l (ny+1-l) with the velocity
+ * reversed, the pressure kept and T' = max(2 T_wall - T, 200 K) */
+static void bc_wall_iso(ox_ctx *c, int ilat, double *w, double *wa) {
+  if (ilat != 3 && ilat != 4) return;
+  int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz, ng = c->g.ng;
+  for (int k = 1; k <= nz; k++)
+    for (int i = 1; i <= nx; i++)
+      for (int l = 1; l <= ng; l++) {
+        size_t p = gi(c, i, ilat == 3 ? l : ny + 1 - l, k);
+        double rho = rho_from_w(c, w, p);
+        for (int lsp = 1; lsp <= NS; lsp++) WG(wa, p, lsp) = WG(w, p, lsp) / rho;
+      }
+  for (int k = 1; k <= nz; k++)
+    for (int i = 1; i <= nx; i++)
+      for (int l = 1; l <= ng; l++) {
+        size_t p = gi(c, i, ilat == 3 ? l : ny + 1 - l, k), q = gi(c, i, ilat == 3 ? 1 - l : ny + l, k);
+        double rho = rho_from_w(c, w, p);
+        double uu = WG(w, p, I_U) / rho, vv = WG(w, p, I_V) / rho, ww = WG(w, p, I_W) / rho;
+        double rhoe = WG(w, p, I_E);
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double ee = rhoe / rho - qq;
+        double Y[MAXNS];
+        for (int lsp = 1; lsp <= NS; lsp++) Y[lsp - 1] = WG(wa, p, lsp);
+        double tt = temperature_from_poly(c, c->cv, ee, WG(wa, p, J_T), Y);
+        double rmixtloc = rmix_wa(c, wa, p);
+        double pp = rho * tt * rmixtloc;
+        tt = 2.0 * c->p.T_wall - tt;
+        if (tt < 200.0) tt = 200.0;
+        ee = mixture_e_wa(c, tt, wa, p);
+        rho = pp / tt / rmixtloc;
+        for (int lsp = 1; lsp <= NS; lsp++) WG(w, q, lsp) = rho * WG(wa, p, lsp);
+        WG(w, q, I_U) = -rho * uu;
+        WG(w, q, I_V) = -rho * vv;
+        WG(w, q, I_W) = -rho * ww;
+        WG(w, q, I_E) = rho * (ee + qq);
+      }
+}
+
 /* update_ghost (multideal_gpu.F90:1165-1238) for tags 0 (nothing), 1 (bcfree_cuf
- * :5073-5100, left side only), 2 (bcextr_cuf :5209-5288), 8 (bcwall_ad_cuf :5749-5852) */
-void ox_update_ghost(ox_ctx *c, double *w, int do_swap) {
+ * :5073-5100, left side only), 2 (bcextr_cuf :5209-5288), 4 (bcextr_sub_cuf
+ * :4092-4327), 5 (bcsym_cuf :5395-5435, y sides only), 6 (bcwall_cuf :5437-5545),
+ * 7 (bcoutopenfoam_cuf :5290-5393), 8 (bcwall_ad_cuf :5749-5852).  Tags 4 and 6
+ * need w_aux (the mass fractions they write back, the Newton guess of tag 6). */
+void ox_update_ghost_aux(ox_ctx *c, double *w, double *wa, int do_swap) {
   int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz, ng = c->g.ng, nv = c->nv;
   for (int ilat = 1; ilat <= 6; ilat++) {
     int tag = c->p.bctags[ilat - 1];
+    if (tag == 4) { bc_extr_sub(c, ilat, w, wa); continue; }
+    if (tag == 6) { bc_wall_iso(c, ilat, w, wa); continue; }
+    if (tag == 5) {
+      /* symmetry about the first (last) row: the y velocity there is set to zero,
+       * ghost 1-l mirrors row l on the lower side, ghost ny+l mirrors ny-l on the upper */
+      if (ilat != 3 && ilat != 4) continue;
+      for (int k = 1; k <= nz; k++)
+        for (int i = 1; i <= nx; i++) {
+          WG(w, gi(c, i, ilat == 3 ? 1 : ny, k), I_V) = 0.0;
+          for (int l = 1; l <= ng; l++) {
+            size_t q = gi(c, i, ilat == 3 ? 1 - l : ny + l, k), p = gi(c, i, ilat == 3 ? l : ny - l, k);
+            for (int lsp = 1; lsp <= NS; lsp++) WG(w, q, lsp) = WG(w, p, lsp);
+            WG(w, q, I_U) = WG(w, p, I_U);
+            WG(w, q, I_V) = -WG(w, p, I_V);
+            WG(w, q, I_W) = WG(w, p, I_W);
+            WG(w, q, I_E) = WG(w, p, I_E);
+          }
+        }
+      continue;
+    }
+    if (tag == 7) {
+      /* zero-gradient outflow; the normal momentum's ghosts are zero where the
+       * boundary cell's flow enters the domain.  The lower z side tests the x
+       * momentum (as the reference does). */
+      int dir = (ilat - 1) / 2, hi = (ilat - 1) % 2;
+      int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+      int na = dir == 0 ? ny : nx, nb = dir == 2 ? ny : nz;
+      int mn = I_U + dir, mtest = ilat == 5 ? I_U : mn;
+      for (int b = 1; b <= nb; b++)
+        for (int a = 1; a <= na; a++) {
+          size_t p = face_pt(c, ilat, a, b, hi ? n : 1);
+          int enter = hi ? WG(w, p, mtest) < 0.0 : WG(w, p, mtest) > 0.0;
+          for (int l = 1; l <= ng; l++) {
+            size_t q = face_pt(c, ilat, a, b, hi ? n + l : 1 - l);
+            for (int m = 1; m <= nv; m++) WG(w, q, m) = (m == mn && enter) ? 0.0 : WG(w, p, m);
+          }
+        }
+      continue;
+    }
     if (tag == 1 && ilat == 1 && c->p.winf) {
       for (int k = 1; k <= nz; k++) for (int j = 1; j <= ny; j++) for (int l = 1; l <= ng; l++)
         for (int m = 1; m <= nv; m++) WG(w, gi(c, 1 - l, j, k), m) = c->p.winf[m - 1];
@@ -487,6 +636,7 @@ void ox_update_ghost(ox_ctx *c, double *w, int do_swap) {
   }
   if (do_swap == 1) ox_bcswap(c, w, c->nv);
 }
+void ox_update_ghost(ox_ctx *c, double *w, int do_swap) { ox_update_ghost_aux(c, w, NULL, do_swap); }
 
 /* ---------------------------------------------------------------- Euler fluxes */
 /* Roe state, compute_roe_average (kernels_gpu.F90:2986-3295) between points p and q */
@@ -1139,6 +1289,90 @@ void ox_visflx(ox_ctx *c, const double *wa, double *fl, double *fhat, int mode) 
 }
 
 /* ---------------------------------------------------------------- RK bookkeeping */
+/* bc_nr (multideal_gpu.F90:1116-1163) with bc_nr_lat_{x,y,z}_kernel
+ * (kernels_gpu.F90:4330-4793): the characteristic boundary treatment of the
+ * boundary cells of every face with bctags_nr > 0.  The one-sided derivative of
+ * the conservative variables, projected on the left eigenvectors of the cell's
+ * state, has its wave amplitudes modified (1: incoming acoustic waves killed;
+ * 2 / 3: incoming waves from the difference to the outer ghost / to winf; 6: a
+ * reflecting wall, entropy and shear waves zero and the incoming acoustic wave
+ * equal to the outgoing one), and the projection back adds to fl. */
+void ox_bc_nr(ox_ctx *c, const double *wa, const double *w, double *fl) {
+  int nv = c->nv;
+  double *el = (double *)malloc(sizeof(double) * nv * nv), *er = (double *)malloc(sizeof(double) * nv * nv);
+  const double c_one[3] = {-1.5, 2.0, -0.5};
+  for (int ilat = 1; ilat <= 6; ilat++) {
+    int nr_type = c->p.bctags_nr[ilat - 1];
+    if (nr_type <= 0) continue;
+    int dir = (ilat - 1) / 2, se = (ilat - 1) % 2 + 1;
+    int n = dir == 0 ? c->g.nx : (dir == 1 ? c->g.ny : c->g.nz);
+    int na = dir == 0 ? c->g.ny : c->g.nx, nb = dir == 2 ? c->g.ny : c->g.nz;
+    int ib = se == 1 ? 1 : n, sgn = se == 1 ? 1 : -1;
+    const double *met = dir == 0 ? c->g.dcsidx : (dir == 1 ? c->g.detady : c->g.dzitdz);
+    for (int b = 1; b <= nb; b++)
+      for (int a = 1; a <= na; a++) {
+        double dw[MAXNS + 4], dwo[MAXNS + 4], dwc[MAXNS + 4], dwco[MAXNS + 4], ev[MAXNS + 4];
+        size_t p = face_pt(c, ilat, a, b, ib);
+        for (int m = 1; m <= nv; m++) {
+          dw[m - 1] = 0.0;
+          for (int l = 1; l <= 3; l++) dw[m - 1] = dw[m - 1] + sgn * c_one[l - 1] * WG(w, face_pt(c, ilat, a, b, ib + sgn * (l - 1)), m);
+          double w_target = 0.0;
+          if (nr_type == 2) w_target = WG(w, face_pt(c, ilat, a, b, ib - sgn), m);
+          else if (nr_type == 3) w_target = c->p.winf ? c->p.winf[m - 1] : 0.0;
+          dwo[m - 1] = sgn * (WG(w, p, m) - w_target);
+        }
+        roe_t R;
+        for (int lsp = 1; lsp <= NS; lsp++) R.yy[lsp - 1] = WG(wa, p, lsp);
+        double rho = WG(wa, p, J_R), uu = WG(wa, p, J_U), vv = WG(wa, p, J_V), ww = WG(wa, p, J_W);
+        double h = WG(wa, p, J_H), tt = WG(wa, p, J_T), pp = WG(wa, p, J_P), cs = WG(wa, p, J_C);
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double cc = cs * cs, rmix_tt = pp / rho, gamloc = cc / rmix_tt, gm1loc = gamloc - 1.0;
+        double p_e = rho * gm1loc, etot = h - rmix_tt;
+        R.b3 = etot;
+        R.b2 = p_e / (rho * cc);
+        R.b1 = -R.b2 * (etot - 2.0 * qq);
+        for (int lsp = 1; lsp <= NS; lsp++) {
+          double eei = species_poly_int(c, c->cv, tt, lsp);
+          R.prhoi[lsp - 1] = c->rgas[lsp - 1] * tt + gm1loc * (etot - qq - eei);
+        }
+        R.rho = rho; R.uu = uu; R.vv = vv; R.ww = ww; R.c = cs; R.ci = 1.0 / cs; R.h = h;
+        eigenvectors(c, dir, &R, el, er);
+        for (int m = 1; m <= nv; m++) {
+          dwc[m - 1] = 0.0;
+          dwco[m - 1] = 0.0;
+          for (int mm = 1; mm <= nv; mm++) {
+            dwc[m - 1] = dwc[m - 1] + el[(size_t)(m - 1) * nv + mm - 1] * dw[mm - 1];
+            dwco[m - 1] = dwco[m - 1] + el[(size_t)(m - 1) * nv + mm - 1] * dwo[mm - 1];
+          }
+        }
+        double un = dir == 0 ? uu : (dir == 1 ? vv : ww);
+        ev[0] = un - cs;
+        for (int lsp = 2; lsp <= NS + 3; lsp++) ev[lsp - 1] = un;
+        ev[NS + 3] = un + cs;
+        if (nr_type == 1)
+          for (int l = 1; l <= nv; l++) ev[l - 1] = sgn * dmin(sgn * ev[l - 1], 0.0);
+        if (nr_type == 2 || nr_type == 3)
+          for (int m = 1; m <= nv; m++)
+            if (sgn * ev[m - 1] > 0.0) dwc[m - 1] = dwco[m - 1];
+        for (int m = 1; m <= nv; m++) dwc[m - 1] = ev[m - 1] * dwc[m - 1];
+        if (nr_type == 6) {
+          for (int lsp = 2; lsp <= NS + 3; lsp++) dwc[lsp - 1] = 0.0;
+          if (se == 1) dwc[NS + 3] = dwc[0];
+          else dwc[0] = dwc[NS + 3];
+        }
+        int ii = dir == 0 ? ib : a, jj = dir == 1 ? ib : (dir == 0 ? a : b), kk = dir == 2 ? ib : b;
+        size_t q = fi(c, ii, jj, kk);
+        for (int m = 1; m <= nv; m++) {
+          double df = 0.0;
+          for (int mm = 1; mm <= nv; mm++) df = df + er[(size_t)(m - 1) * nv + mm - 1] * dwc[mm - 1];
+          fl[q + (size_t)(m - 1) * c->npi] = fl[q + (size_t)(m - 1) * c->npi] + df * met[ib - 1];
+        }
+      }
+  }
+  free(el);
+  free(er);
+}
+
 void ox_init_flux(ox_ctx *c, double *fl, double *fln, double rhodt) {
   size_t n = c->npi * c->nv;
 #pragma omp parallel for schedule(static)
@@ -1198,6 +1432,29 @@ void ox_compute_dt(ox_ctx *c, const double *wa, const int32_t *mask, double out9
         for (int q = 0; q < 9; q++) mx[q] = dmax(mx[q], v[q]);
       }
   for (int q = 0; q < 9; q++) out9[q] = mx[q];
+}
+
+/* compute_residual_cuf + compute_rho_t_p_minmax_cuf (kernels_gpu.F90:5991-6011,
+ * 6038-6073) and the residual's normalisation (multideal_gpu.F90:1603-1606):
+ * out7 = {residual_rhou, rhomin, rhomax, tmin, tmax, pmin, pmax}. */
+void ox_compute_residual(ox_ctx *c, const double *fln, const double *wa, const int32_t *mask, double dt,
+                         double out7[7]) {
+  int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz;
+  double res = 0.0;
+  double mn[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, mx[3] = {-100.0, -100.0, -100.0};
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        size_t p = gi(c, i, j, k);
+        if (mask != NULL && mask[p] != 0) continue;
+        size_t q = (size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1));
+        double f = fln[q + (size_t)(I_U - 1) * (size_t)nx * ny * nz] / dt;
+        res = res + f * f;
+        double v[3] = {WG(wa, p, J_R), WG(wa, p, J_T), WG(wa, p, J_P)};
+        for (int l = 0; l < 3; l++) { mn[l] = fmin(mn[l], v[l]); mx[l] = dmax(mx[l], v[l]); }
+      }
+  out7[0] = sqrt(res / ((double)nx * (double)ny * (double)nz));
+  for (int l = 0; l < 3; l++) { out7[1 + 2 * l] = mn[l]; out7[2 + 2 * l] = mx[l]; }
 }
 
 /* ---------------------------------------------------------------- chemistry */
@@ -1904,11 +2161,12 @@ void ox_rk_sync(ox_ctx *c, const stx_fields *f, double *fhat, double dt, int sim
       ox_visflx(c, f->w_aux, f->fl, fhat, 1);
       ox_visflx(c, f->w_aux, f->fl, fhat, 2);
     }
+    ox_bc_nr(c, f->w_aux, f->w, f->fl);
     if (c->p.enable_chemistry == 1) ox_compute_chemistry(c, f->w, f->w_aux, f->fl);
     if (simpler == 1) ox_update_simpler_flux(c, f->fl, f->fln, f->fl_sav, gamdt);
     else ox_update_flux(c, f->fl, f->fln, gamdt);
     ox_update_field(c, f->w, f->fln, f->fluid_mask);
-    ox_update_ghost(c, f->w, 0);
+    ox_update_ghost_aux(c, f->w, f->w_aux, 0);
   }
 }
 
@@ -1927,8 +2185,9 @@ static void ox_sav_flx_step(ox_ctx *c, const stx_fields *f, double *fhat) {
     ox_visflx(c, f->w_aux, f->fl, fhat, 1);
     ox_visflx(c, f->w_aux, f->fl, fhat, 2);
   }
+  ox_bc_nr(c, f->w_aux, f->w, f->fl);
   if (c->p.enable_chemistry == 1) ox_compute_chemistry(c, f->w, f->w_aux, f->fl);
-  ox_update_ghost(c, f->w, 0);
+  ox_update_ghost_aux(c, f->w, f->w_aux, 0);
   ox_sav_flx(c, f->fl, f->fl_sav);
 }
 

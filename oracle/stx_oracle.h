@@ -35,6 +35,10 @@ void ox_eval_aux2(ox_ctx *c, double *w_aux);
 void ox_bcextr_var(ox_ctx *c, double *var);
 void ox_bcswap(ox_ctx *c, double *field, int nvar);
 void ox_update_ghost(ox_ctx *c, double *w, int do_swap);
+void ox_update_ghost_aux(ox_ctx *c, double *w, double *w_aux, int do_swap);
+void ox_bc_nr(ox_ctx *c, const double *w_aux, const double *w, double *fl);
+void ox_compute_residual(ox_ctx *c, const double *fln, const double *wa, const int32_t *mask, double dt,
+                         double out7[7]);
 /* face fluxes into fhat (ghosted, nv) for faces [face_lo, face_hi], then the update over [imin, imax] */
 void ox_euler(ox_ctx *c, int dir, const double *w_aux, double *fhat, double *fl, int nmin, int nmax);
 void ox_visflx(ox_ctx *c, const double *w_aux, double *fl, double *fhat, int mode);

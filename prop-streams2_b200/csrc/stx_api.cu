@@ -19,6 +19,8 @@ struct stx_ctx {
   unsigned int *status_d;         // device status word
   unsigned int *counter_d;        // work-stealing cell counter of the Rosenbrock kernels
   unsigned long long *dt_d;       // the nine CFL maxima
+  double *res_d;                  // residual partial sums (STX_RES_BLOCKS) of stx_compute_residual
+  unsigned long long *mm_d;       // its six rho / T / p extrema
   double *time_d;                 // simulation time of captured steps (stx_graph_*)
   const DevCtx *dctx_d;           // device copy of d, for device functions that take the context by reference
   stx_exchange_fn xfn = nullptr;   // ghost exchange at STX_BC_EXCHANGE faces (stx_set_exchange)
@@ -155,6 +157,9 @@ const char *stx_strerror(int code) {
     case STX_E_NOMEM: return "device allocation failed";
     case STX_E_UNSUPPORTED: return "option outside the supported hot path";
     case STX_E_TOO_LARGE: return "more cells than the allocation-free entry point's fixed scratch allows (2^31)";
+    case STX_E_LOCAL_MEM:
+      return "the device's per-thread stack limit (cudaLimitStackSize) is below the allocation-free kernel's local "
+             "frame; raise it once with cudaDeviceSetLimit before calling";
     default: return "unknown error";
   }
 }
@@ -193,13 +198,25 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   if (par->ep_order / 2 > grid->ng || par->visc_order / 2 > grid->ng || par->weno_scheme > grid->ng) return STX_E_INVALID;
   if (par->nrk < 1 || par->nrk > 4) return STX_E_INVALID;
   for (int q = 0; q < 6; q++) {
-    int t = par->bctags[q];
-    if (t != 0 && t != 1 && t != 2 && t != 8 && t != STX_BC_EXCHANGE) return STX_E_UNSUPPORTED;
-    if (par->bctags_nr[q] != 0) return STX_E_UNSUPPORTED;
+    int t = par->bctags[q], nr = par->bctags_nr[q];
+    // update_ghost tags of this path (multideal_gpu.F90:1176-1233); 9 (laminar-profile
+    // inflow), 10 (recycling), 26/28 (jets) and 46/56 (special walls) are not
+    if (t != 0 && t != 1 && t != 2 && t != 4 && t != 5 && t != 6 && t != 7 && t != 8 && t != STX_BC_EXCHANGE)
+      return STX_E_UNSUPPORTED;
+    if (nr != 0 && nr != 1 && nr != 2 && nr != 3 && nr != 6) return STX_E_UNSUPPORTED;
+    if (nr != 0 && (t == 0 || t == STX_BC_EXCHANGE)) return STX_E_INVALID;   // no characteristic face inside the domain
+    if (nr == 3 && !par->winf) return STX_E_INVALID;
   }
-  if (par->eul_imin != 1 || par->eul_imax != grid->nx || par->eul_jmin != 1 || par->eul_jmax != grid->ny ||
-      par->eul_kmin != 1 || par->eul_kmax != grid->nz)
-    return STX_E_UNSUPPORTED;
+  // bc_preproc (multideal.F90:5671-5718): a face with a characteristic treatment
+  // leaves its boundary cells out of the convective flux divergence
+  {
+    const int lo[3] = {1, 1, 1}, hi[3] = {grid->nx, grid->ny, grid->nz};
+    const int got[6] = {par->eul_imin, par->eul_imax, par->eul_jmin, par->eul_jmax, par->eul_kmin, par->eul_kmax};
+    for (int q = 0; q < 6; q++) {
+      int want = (q % 2 == 0 ? lo[q / 2] : hi[q / 2]) + (par->bctags_nr[q] != 0 ? (q % 2 == 0 ? 1 : -1) : 0);
+      if (got[q] != want) return STX_E_UNSUPPORTED;
+    }
+  }
   if (!base && (tab->nsetcv < 1 || tab->num_t_tab < 1)) return STX_E_INVALID;
   if (par->enable_chemistry > 0 && nr < 1) return STX_E_INVALID;
   stx_ctx *c = new (std::nothrow) stx_ctx();
@@ -371,6 +388,7 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   p.nv_aux = par->nv_aux;
   for (int q = 0; q < 6; q++) p.fzf[q] = par->force_zero_flux[q];
   p.ros_maxsteps = par->ros_maxsteps; p.ros_maxtry = par->ros_maxtry;
+  p.T_wall = par->T_wall;
   std::memset(p.cd1, 0, sizeof(p.cd1));
   // coeff_deriv1 (src/grid.F90:135-160), column lmax = order/2
   p.cd1[1][1] = 0.5;
@@ -385,6 +403,12 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   if ((rc = upload<unsigned long long>(c, nullptr, 9, &dtp))) return fail(rc);
   const double *tm = nullptr;
   if ((rc = upload<double>(c, nullptr, 1, &tm))) return fail(rc);
+  const double *rp = nullptr;
+  const unsigned long long *mmp = nullptr;
+  if ((rc = upload<double>(c, nullptr, STX_RES_BLOCKS, &rp))) return fail(rc);
+  if ((rc = upload<unsigned long long>(c, nullptr, 6, &mmp))) return fail(rc);
+  c->res_d = (double *)rp;
+  c->mm_d = (unsigned long long *)mmp;
   c->status_d = (unsigned int *)st;
   c->counter_d = (unsigned int *)cn;
   c->dt_d = (unsigned long long *)dtp;
@@ -507,16 +531,34 @@ int stx_set_exchange(stx_ctx *c, stx_exchange_fn fn, void *user) {
   return STX_OK;
 }
 
-int stx_update_ghost(stx_ctx *c, void *s, double *w, int do_swap) {
+int stx_update_ghost_aux(stx_ctx *c, void *s, double *w, double *w_aux, int do_swap) {
   if (!c || !w) return STX_E_INVALID;
   for (int ilat = 1; ilat <= 6; ilat++) {
     int tag = c->par.bctags[ilat - 1];
-    if (tag == 1 || tag == 2 || tag == 8) {
+    if (tag == 1 || tag == 2 || tag == 5 || tag == 7 || tag == 8) {
       Prof pf(c, S(s), STX_K_GHOST, 1);
       TRY(launch_bc_face(c->d, S(s), w, ilat, tag, c->winf_d));
+    } else if (tag == 4 || tag == 6) {
+      if (!w_aux) return STX_E_INVALID;              // these fills read and write w_aux
+      Prof pf(c, S(s), STX_K_GHOST, 1);
+      TRY(launch_bc_face_thermo(c->d, S(s), w, w_aux, ilat, tag));
     }
   }
   if (do_swap == 1) TRY(stx_bcswap(c, s, w, c->nv));
+  return STX_OK;
+}
+int stx_update_ghost(stx_ctx *c, void *s, double *w, int do_swap) {
+  return stx_update_ghost_aux(c, s, w, nullptr, do_swap);
+}
+
+int stx_bc_nr(stx_ctx *c, void *s, const double *w_aux, const double *w, double *fl) {
+  if (!c || !w_aux || !w || !fl) return STX_E_INVALID;
+  for (int ilat = 1; ilat <= 6; ilat++) {
+    int nr = c->par.bctags_nr[ilat - 1];
+    if (nr <= 0) continue;
+    Prof pf(c, S(s), STX_K_EULER, 1);
+    TRY(launch_bc_nr(c->d, S(s), w_aux, w, fl, c->winf_d, ilat, nr));
+  }
   return STX_OK;
 }
 
@@ -611,6 +653,27 @@ int stx_compute_dt(stx_ctx *c, void *s, const double *wa, const int32_t *mask, d
   return STX_OK;
 }
 
+int stx_compute_residual(stx_ctx *c, void *s, const double *fln, const double *wa, const int32_t *mask, double dt,
+                         double out7[7]) {
+  if (!c || !fln || !wa || !out7 || !(dt != 0.0)) return STX_E_INVALID;
+  {
+    Prof pf(c, S(s), STX_K_DT, 1, (double)c->d.g.npi * B8(4));
+    TRY(launch_residual_minmax(c->d, S(s), fln, wa, mask, dt, c->res_d, c->mm_d));
+  }
+  double part[STX_RES_BLOCKS];
+  unsigned long long h[6];
+  STX_CUDA_TRY(cudaMemcpyAsync(part, c->res_d, sizeof(part), cudaMemcpyDeviceToHost, S(s)));
+  STX_CUDA_TRY(cudaMemcpyAsync(h, c->mm_d, sizeof(h), cudaMemcpyDeviceToHost, S(s)));
+  STX_CUDA_TRY(cudaStreamSynchronize(S(s)));
+  double sum = 0.0;
+  for (int b = 0; b < STX_RES_BLOCKS; b++) sum = sum + part[b];
+  // residual_rhou = sqrt(sum / (nx ny nz nprocs)) (multideal_gpu.F90:1603-1606, one process)
+  out7[0] = std::sqrt(sum / ((double)c->d.g.nx * (double)c->d.g.ny * (double)c->d.g.nz));
+  const int order[6] = {0, 3, 1, 4, 2, 5};     // rhomin, rhomax, tmin, tmax, pmin, pmax
+  for (int q = 0; q < 6; q++) std::memcpy(&out7[1 + q], &h[order[q]], sizeof(double));
+  return STX_OK;
+}
+
 // ------------------------------------------------------------------ chemistry
 int stx_rosenbrock(stx_ctx *c, void *s, double *w, double *wa, double dttry, double t0, double t1) {
   if (!c || !w || !wa) return STX_E_INVALID;
@@ -623,7 +686,7 @@ int stx_rosenbrock_krylov(stx_ctx *c, void *s, double *w, const double *wa, cons
   if (!c || !w || !wa || (simpler == 1 && !fl_sav)) return STX_E_INVALID;
   if (c->d.t.nr < 1) return STX_E_INVALID;
   Prof pf(c, S(s), STX_K_CHEM, 1, (double)c->d.g.npi * B8(2 * c->nv + 2));
-  return launch_rok4(c->d, S(s), w, wa, fl_sav, dttry, t0, t1, simpler, c->counter_d);
+  return launch_rok4(c->d, c->dctx_d, S(s), w, wa, fl_sav, dttry, t0, t1, simpler, c->counter_d);
 }
 int stx_batch0d_integrate(stx_ctx *c, void *s, int n, const double *T0, const double *p0, const double *Y0,
                           double t_max, double dttry, double ign_factor, double end_factor, int max_steps, double *Y,
@@ -646,8 +709,8 @@ int stx_batch0d_integrate(stx_ctx *c, void *s, int n, const double *T0, const do
                                  nsteps, c->counter_d, force);
     if (rc != STX_E_UNSUPPORTED) return rc;
   }
-  return launch_batch0d(d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end, nsteps,
-                        c->counter_d);
+  return launch_batch0d(d, c->dctx_d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end,
+                        nsteps, c->counter_d);
 }
 int stx_compute_chemistry(stx_ctx *c, void *s, double *w, double *wa, double *fl) {
   if (!c || !w || !wa || !fl) return STX_E_INVALID;
@@ -672,6 +735,7 @@ static int rhs_pass(stx_ctx *c, void *s, const stx_fields *f) {
   if (g.nz > 1) TRY(stx_euler_z(c, s, f->w_aux, f->fl, c->par.eul_kmin, c->par.eul_kmax, 0));
   TRY(stx_visflx(c, s, f->w_aux, f->fl, 1));
   TRY(stx_visflx(c, s, f->w_aux, f->fl, 2));
+  TRY(stx_bc_nr(c, s, f->w_aux, f->w, f->fl));
   if (c->par.enable_chemistry == 1) TRY(stx_compute_chemistry(c, s, f->w, f->w_aux, f->fl));
   return STX_OK;
 }
@@ -685,7 +749,7 @@ int stx_rk_sync(stx_ctx *c, void *s, const stx_fields *f, double dt, int simpler
     else TRY(stx_init_flux(c, s, f->fl, f->fln, rhodt));
     TRY(rhs_pass(c, s, f));
     TRY(stx_rk_finish(c, s, f->w, f->fl, f->fln, f->fl_sav, f->fluid_mask, gamdt, simpler));
-    TRY(stx_update_ghost(c, s, f->w, 0));
+    TRY(stx_update_ghost_aux(c, s, f->w, f->w_aux, 0));
   }
   return STX_OK;
 }
@@ -700,7 +764,7 @@ int stx_advance_solution(stx_ctx *c, void *s, const stx_fields *f, double dt, do
       // sav_flx (multideal_gpu.F90:623-692): fl = 0, one right-hand side, fl_sav = fl
       STX_CUDA_TRY(cudaMemsetAsync(f->fl, 0, sizeof(double) * c->d.g.npi * c->nv, S(s)));
       TRY(rhs_pass(c, s, f));
-      TRY(stx_update_ghost(c, s, f->w, 0));
+      TRY(stx_update_ghost_aux(c, s, f->w, f->w_aux, 0));
       TRY(stx_sav_flx(c, s, f->fl, f->fl_sav));
       TRY(stx_compute_aux(c, s, f->w, f->w_aux, 1, 0));
       TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, f->fl_sav, dt_chem, time, time + dt_chem, 1));
@@ -934,7 +998,7 @@ int stx_autotune(stx_ctx *c, void *sv, const stx_fields *f, double dt_chem, stx_
         float ms = time_launches(s, e0, e1, 1, [&] {
           if (cudaMemcpyAsync(w2, f->w, nw * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             return (int)STX_E_CUDA;
-          return launch_rok4(c->d, s, w2, f->w_aux, nullptr, dt_chem, 0.0, dt_chem, 0, c->counter_d);
+          return launch_rok4(c->d, c->dctx_d, s, w2, f->w_aux, nullptr, dt_chem, 0.0, dt_chem, 0, c->counter_d);
         });
         if (ms < 0.f) { rc = STX_E_CUDA; break; }
         if (best < 0.f || ms < 0.95f * best) { best = ms; pick = k; }

@@ -245,8 +245,14 @@ __global__ void k_bcswap(DevCtx c, double *__restrict__ f, int nvar, int px, int
   }
 }
 
-// update_ghost face kernels: bcfree_cuf (:5073, left side), bcextr_cuf (:5209),
-// bcwall_ad_cuf (:5749).  One launch per face, faces in the reference's order.
+// update_ghost face kernels without thermodynamics, one thread per (variable,
+// boundary point), all ng ghost layers: bcfree_cuf (kernels_gpu.F90:5073, left
+// side), bcextr_cuf (:5209), bcsym_cuf (:5395, y sides: the normal velocity of
+// the first / last row set to zero, ghosts mirrored about row 1 / row ny with
+// the normal momentum reversed), bcoutopenfoam_cuf (:5290: zero-gradient, with
+// the normal momentum's ghosts zero where the boundary cell's flow enters; the
+// lower z side tests the x momentum, as the reference does), bcwall_ad_cuf
+// (:5749).  One launch per face, faces in the reference's order.
 __global__ void k_bc_face(DevCtx c, double *__restrict__ w, int ilat, int tag, int nv, const double *__restrict__ winf) {
   const DevGrid &g = c.g;
   int dir = (ilat - 1) / 2, hi = (ilat - 1) % 2;
@@ -259,19 +265,284 @@ __global__ void k_bc_face(DevCtx c, double *__restrict__ w, int ilat, int tag, i
   int a = 1 + (int)(q % na), b = 1 + (int)(q / na);
   int n = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
   int ns = nv - 4;
+  auto at = [&](int nn) -> long long {
+    return dir == 0 ? gidx(g, nn, a, b) : (dir == 1 ? gidx(g, a, nn, b) : gidx(g, a, b, nn));
+  };
+  const int mn = ns + 1 + dir;                       // the normal momentum
   double sg = (tag == 8 && m >= ns + 1 && m <= ns + 3) ? -1.0 : 1.0;
+  bool zero = false;
+  if (tag == 5) {
+    if (dir != 1) return;
+    if (m == mn) FG(w, at(hi ? n : 1), m) = 0.0;
+    if (m == mn) sg = -1.0;
+  } else if (tag == 7 && m == mn) {
+    const int mt = ilat == 5 ? ns + 1 : mn;
+    double v = FG(w, at(hi ? n : 1), mt);
+    zero = hi ? v < 0.0 : v > 0.0;
+  }
   for (int l = 1; l <= g.ng; l++) {
     int dst = hi ? n + l : 1 - l;
     int src;
-    if (tag == 2) src = hi ? n : 1;
+    if (tag == 2 || tag == 7) src = hi ? n : 1;
+    else if (tag == 5) src = hi ? n - l : l;
     else src = hi ? n + 1 - l : l;   // tag 8
-    int id[3], is[3];
-    if (dir == 0) { id[0] = dst; id[1] = a; id[2] = b; is[0] = src; is[1] = a; is[2] = b; }
-    else if (dir == 1) { id[0] = a; id[1] = dst; id[2] = b; is[0] = a; is[1] = src; is[2] = b; }
-    else { id[0] = a; id[1] = b; id[2] = dst; is[0] = a; is[1] = b; is[2] = src; }
-    long long pd = gidx(g, id[0], id[1], id[2]);
+    long long pd = at(dst);
     if (tag == 1) FG(w, pd, m) = winf[m - 1];
-    else FG(w, pd, m) = sg * FG(w, gidx(g, is[0], is[1], is[2]), m);
+    else FG(w, pd, m) = zero ? 0.0 : sg * FG(w, at(src), m);
+  }
+}
+
+// get_mixture_e_from_temperature_dev (kernels_gpu.F90:7047-7102) with the mass
+// fractions Y: the species ranges located at tt, the constants then the
+// integrated terms l = icl..icr, each over the species in order.
+template <int NS>
+__device__ double mix_e_at(const DevTab &t, double tt, const double *Y) {
+  int nrange[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) nrange[k] = t.nset > 1 ? locate_range(t, tt, k + 1) : 1;
+  double ee = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) ee = ee + cpc(t, t.cv, t.icr + 1, k + 1, nrange[k]) * Y[k];
+  for (int l = t.icl; l <= t.icr; l++) {
+    double tprod = l == -1 ? log(tt) : ipow(tt, l + 1) / (l + 1.0);
+    double cv_l = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) cv_l = cv_l + cpc(t, t.cv, l, k + 1, nrange[k]) * Y[k];
+    ee = ee + cv_l * tprod;
+  }
+  return ee;
+}
+
+// update_ghost face kernels that need the thermodynamics and w_aux, one thread
+// per boundary point, all ng layers:
+//  * tag 4, bcextr_sub_cuf (kernels_gpu.F90:4092-4327), every side: the
+//    boundary cell's mass fractions into w_aux; ghosts with its species and
+//    momentum and the energy at T = p0 / (rho R_mix);
+//  * tag 6, bcwall_cuf (:5437-5545), y sides only: the first ng interior rows'
+//    mass fractions into w_aux; ghost 1-l (ny+l) mirrors row l (ny+1-l) with the
+//    velocity reversed, the pressure kept and T' = max(2 T_wall - T, 200 K), T
+//    from e by the Newton iteration started at the row's w_aux(J_T).
+template <int NS>
+__global__ void k_bc_face_thermo(DevCtx c, double *__restrict__ w, double *__restrict__ wa, int ilat, int tag) {
+  const DevGrid &g = c.g;
+  const DevTab &t = c.t;
+  int dir = (ilat - 1) / 2, hi = (ilat - 1) % 2;
+  int na = dir == 0 ? g.ny : g.nx, nb = dir == 2 ? g.ny : g.nz;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)na * nb) return;
+  int a = 1 + (int)(tid % na), b = 1 + (int)(tid / na);
+  int n = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
+  auto at = [&](int nn) -> long long {
+    return dir == 0 ? gidx(g, nn, a, b) : (dir == 1 ? gidx(g, a, nn, b) : gidx(g, a, b, nn));
+  };
+  if (tag == 4) {
+    long long p = at(hi ? n : 1);
+    double rho = FG(w, p, 1);
+#pragma unroll
+    for (int k = 1; k < NS; k++) rho = rho + FG(w, p, k + 1);
+    double Y[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) { Y[k] = FG(w, p, k + 1) / rho; FG(wa, p, k + 1) = Y[k]; }
+    double rm = ldg(t.rgas) * Y[0];
+#pragma unroll
+    for (int k = 1; k < NS; k++) rm = rm + ldg(t.rgas + k) * Y[k];
+    const double tt = c.p.p0 / rho / rm;
+    const double ee = mix_e_at<NS>(t, tt, Y);
+    const double rhou = FG(w, p, NS + 1), rhov = FG(w, p, NS + 2), rhow = FG(w, p, NS + 3);
+    const double rhoE = rho * ee + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
+    for (int l = 1; l <= g.ng; l++) {
+      long long q = at(hi ? n + l : 1 - l);
+#pragma unroll
+      for (int k = 0; k < NS; k++) FG(w, q, k + 1) = FG(w, p, k + 1);
+      FG(w, q, NS + 1) = rhou;
+      FG(w, q, NS + 2) = rhov;
+      FG(w, q, NS + 3) = rhow;
+      FG(w, q, NS + 4) = rhoE;
+    }
+    return;
+  }
+  // tag 6 (the host launches it for the y sides only)
+  for (int l = 1; l <= g.ng; l++) {
+    long long p = at(hi ? n + 1 - l : l);
+    double rho = FG(w, p, 1);
+#pragma unroll
+    for (int k = 1; k < NS; k++) rho = rho + FG(w, p, k + 1);
+#pragma unroll
+    for (int k = 0; k < NS; k++) FG(wa, p, k + 1) = FG(w, p, k + 1) / rho;
+  }
+  for (int l = 1; l <= g.ng; l++) {
+    long long p = at(hi ? n + 1 - l : l), q = at(hi ? n + l : 1 - l);
+    double rho = FG(w, p, 1);
+#pragma unroll
+    for (int k = 1; k < NS; k++) rho = rho + FG(w, p, k + 1);
+    double uu = FG(w, p, NS + 1) / rho, vv = FG(w, p, NS + 2) / rho, ww = FG(w, p, NS + 3) / rho;
+    double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+    double ee = FG(w, p, NS + 4) / rho - qq;
+    double Y[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) Y[k] = FG(wa, p, k + 1);
+    double tt = temp_from_e<NS>(t, c.p, ee, FG(wa, p, NS + 5), Y);
+    double rm = ldg(t.rgas) * Y[0];
+#pragma unroll
+    for (int k = 1; k < NS; k++) rm = rm + ldg(t.rgas + k) * Y[k];
+    double pp = rho * tt * rm;
+    tt = 2.0 * c.p.T_wall - tt;
+    if (tt < 200.0) tt = 200.0;
+    ee = mix_e_at<NS>(t, tt, Y);
+    rho = pp / tt / rm;
+#pragma unroll
+    for (int k = 0; k < NS; k++) FG(w, q, k + 1) = rho * Y[k];
+    FG(w, q, NS + 1) = -rho * uu;
+    FG(w, q, NS + 2) = -rho * vv;
+    FG(w, q, NS + 3) = -rho * ww;
+    FG(w, q, NS + 4) = rho * (ee + qq);
+  }
+}
+
+// ---------------------------------------------------------------- characteristic boundaries
+// Entries of the left (el(n, m): variable n, wave m) and right (er(m, n): wave m,
+// variable n) eigenvectors of eigenvectors_{x,y,z} (kernels_gpu.F90:2703-2984),
+// 1-based, formed on the fly from the point state instead of stored as
+// (ns+4)^2 matrices.
+struct NrPoint {
+  double b1, b2, b3, c, ci, cci, h, un, v1, v2, vel[3];
+  int dir, it1, it2;
+};
+template <int NS>
+__device__ __forceinline__ double nr_el(const NrPoint &R, const double *yy, const double *prhoi, int n, int m) {
+  const int In = NS + 1 + R.dir, It1 = NS + 1 + R.it1, It2 = NS + 1 + R.it2, IE = NS + 4;
+  if (n <= NS) {
+    const double b1n = R.b1 + prhoi[n - 1] * R.cci;
+    if (m == 1) return 0.5 * (b1n + R.un * R.ci);
+    if (m <= NS + 1) return (n == m - 1 ? 1.0 : 0.0) - b1n * yy[m - 2];
+    if (m == NS + 2) return -R.v1;
+    if (m == NS + 3) return -R.v2;
+    return 0.5 * (b1n - R.un * R.ci);
+  }
+  if (m >= 2 && m <= NS + 1) return n == IE ? -R.b2 * yy[m - 2] : R.b2 * R.vel[n - NS - 1] * yy[m - 2];
+  if (m == 1) {
+    if (n == In) return -0.5 * (R.b2 * R.un + R.ci);
+    if (n == It1) return -0.5 * (R.b2 * R.v1);
+    if (n == It2) return -0.5 * (R.b2 * R.v2);
+    return 0.5 * R.b2;
+  }
+  if (m == NS + 2) return n == It1 ? 1.0 : 0.0;
+  if (m == NS + 3) return n == It2 ? 1.0 : 0.0;
+  if (n == In) return -0.5 * (R.b2 * R.un - R.ci);
+  if (n == It1) return -0.5 * (R.b2 * R.v1);
+  if (n == It2) return -0.5 * (R.b2 * R.v2);
+  return 0.5 * R.b2;
+}
+template <int NS>
+__device__ __forceinline__ double nr_er(const NrPoint &R, const double *yy, const double *prhoi, int m, int n) {
+  const int In = NS + 1 + R.dir, It1 = NS + 1 + R.it1, It2 = NS + 1 + R.it2, IE = NS + 4;
+  if (n <= NS) {                                       // species columns
+    if (m == 1 || m == NS + 4) return yy[n - 1];
+    return m == n + 1 ? 1.0 : 0.0;
+  }
+  if (m >= 2 && m <= NS + 1) {                         // species waves
+    if (n == IE) return R.b3 - prhoi[m - 2] / R.b2 * R.cci;
+    return R.vel[n - NS - 1];
+  }
+  if (m == 1) {
+    if (n == In) return R.un - R.c;
+    if (n == It1) return R.v1;
+    if (n == It2) return R.v2;
+    return R.h - R.un * R.c;
+  }
+  if (m == NS + 2) return n == It1 ? 1.0 : (n == IE ? R.v1 : 0.0);
+  if (m == NS + 3) return n == It2 ? 1.0 : (n == IE ? R.v2 : 0.0);
+  if (n == In) return R.un + R.c;
+  if (n == It1) return R.v1;
+  if (n == It2) return R.v2;
+  return R.h + R.un * R.c;
+}
+
+// bc_nr_lat_{x,y,z}_kernel (kernels_gpu.F90:4330-4793), one thread per boundary
+// cell of face ilat: the one-sided derivative of w projected on the waves, the
+// wave amplitudes of treatment nr_type (1 incoming acoustic waves removed; 2 / 3
+// incoming waves from the difference to the outer ghost / to winf; 6 reflecting
+// wall), projected back and added to fl.
+template <int NS>
+__global__ void k_bc_nr(DevCtx c, const double *__restrict__ wa, const double *__restrict__ w, double *__restrict__ fl,
+                        const double *__restrict__ winf, int ilat, int nr_type) {
+  constexpr int NV = NS + 4;
+  const DevGrid &g = c.g;
+  const int dir = (ilat - 1) / 2, se = (ilat - 1) % 2 + 1;
+  const int na = dir == 0 ? g.ny : g.nx, nb = dir == 2 ? g.ny : g.nz;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)na * nb) return;
+  const int a = 1 + (int)(tid % na), b = 1 + (int)(tid / na);
+  const int n = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
+  const int ib = se == 1 ? 1 : n, sgn = se == 1 ? 1 : -1;
+  auto at = [&](int nn) -> long long {
+    return dir == 0 ? gidx(g, nn, a, b) : (dir == 1 ? gidx(g, a, nn, b) : gidx(g, a, b, nn));
+  };
+  const double c_one[3] = {-1.5, 2.0, -0.5};
+  const long long p = at(ib);
+  double dw[NV], dwo[NV];
+  for (int m = 1; m <= NV; m++) {
+    double d = 0.0;
+    for (int l = 1; l <= 3; l++) d = d + sgn * c_one[l - 1] * FG(w, at(ib + sgn * (l - 1)), m);
+    dw[m - 1] = d;
+    double w_target = 0.0;
+    if (nr_type == 2) w_target = FG(w, at(ib - sgn), m);
+    else if (nr_type == 3) w_target = winf ? winf[m - 1] : 0.0;
+    dwo[m - 1] = sgn * (FG(w, p, m) - w_target);
+  }
+  double yy[NS], prhoi[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) yy[k] = FG(wa, p, k + 1);
+  const double rho = FG(wa, p, NS + 11), uu = FG(wa, p, NS + 1), vv = FG(wa, p, NS + 2), ww = FG(wa, p, NS + 3);
+  const double h = FG(wa, p, NS + 4), tt = FG(wa, p, NS + 5), pp = FG(wa, p, NS + 6), cs = FG(wa, p, NS + 7);
+  const double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+  const double cc = cs * cs, rmix_tt = pp / rho, gamloc = cc / rmix_tt, gm1loc = gamloc - 1.0;
+  const double p_e = rho * gm1loc, etot = h - rmix_tt;
+  NrPoint R;
+  R.b3 = etot;
+  R.b2 = p_e / (rho * cc);
+  R.b1 = -R.b2 * (etot - 2.0 * qq);
+  for (int k = 0; k < NS; k++) {
+    const double eei = species_poly_int(c.t, c.t.cvi, tt, k + 1);
+    prhoi[k] = ldg(c.t.rgas + k) * tt + gm1loc * (etot - qq - eei);
+  }
+  R.c = cs;
+  R.ci = 1.0 / cs;
+  R.cci = R.ci * R.ci;
+  R.h = h;
+  R.vel[0] = uu; R.vel[1] = vv; R.vel[2] = ww;
+  R.dir = dir;
+  R.it1 = dir == 0 ? 1 : 0;
+  R.it2 = dir == 2 ? 1 : 2;
+  R.un = R.vel[dir];
+  R.v1 = R.vel[R.it1];
+  R.v2 = R.vel[R.it2];
+  double dwc[NV];
+  for (int m = 1; m <= NV; m++) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int mm = 1; mm <= NV; mm++) {
+      const double e = nr_el<NS>(R, yy, prhoi, mm, m);
+      s1 = s1 + e * dw[mm - 1];
+      s2 = s2 + e * dwo[mm - 1];
+    }
+    double ev = (m == 1) ? R.un - cs : (m == NV ? R.un + cs : R.un);
+    if (nr_type == 1) ev = sgn * dmin_(sgn * ev, 0.0);
+    if ((nr_type == 2 || nr_type == 3) && sgn * ev > 0.0) s1 = s2;
+    dwc[m - 1] = ev * s1;
+  }
+  if (nr_type == 6) {
+    for (int m = 2; m <= NS + 3; m++) dwc[m - 1] = 0.0;
+    if (se == 1) dwc[NV - 1] = dwc[0];
+    else dwc[0] = dwc[NV - 1];
+  }
+  const double *met = dir == 0 ? g.dcsidx : (dir == 1 ? g.detady : g.dzitdz);
+  const double mt = ldg(met + ib - 1);
+  const int ii = dir == 0 ? ib : a, jj = dir == 1 ? ib : (dir == 0 ? a : b), kk = dir == 2 ? ib : b;
+  const long long q = fidx(g, ii, jj, kk);
+  for (int m = 1; m <= NV; m++) {
+    double df = 0.0;
+    for (int mm = 1; mm <= NV; mm++) df = df + nr_er<NS>(R, yy, prhoi, mm, m) * dwc[mm - 1];
+    FI(fl, q, m) = FI(fl, q, m) + df * mt;
   }
 }
 
@@ -372,6 +643,59 @@ __global__ void __launch_bounds__(256) k_compute_dt(DevCtx c, const double *__re
   }
 }
 
+// compute_residual_cuf + compute_rho_t_p_minmax_cuf (kernels_gpu.F90:5991-6011,
+// 6038-6073): the sum of (fln(I_U)/dt)^2 and the extrema of rho, T and p over
+// the fluid interior cells.  The sum is deterministic: a fixed grid of
+// RES_BLOCKS blocks, each writing its partial sum (warp shuffles in a fixed
+// order) to part[block]; the host adds the partials in block order.  The
+// extrema of these positive quantities are exact: atomicMin / atomicMax on the
+// bit patterns of the doubles (mm[0..2] minima of rho, T, p; mm[3..5] maxima).
+template <int NS>
+__global__ void __launch_bounds__(256) k_residual_minmax(DevCtx c, const double *__restrict__ fln,
+                                                         const double *__restrict__ wa, const int32_t *__restrict__ mask,
+                                                         double dt, double *__restrict__ part,
+                                                         unsigned long long *__restrict__ mm) {
+  const DevGrid &g = c.g;
+  double sum = 0.0, vmin[3] = {INFINITY, INFINITY, INFINITY}, vmax[3] = {0.0, 0.0, 0.0};
+  for (long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x; tid < g.npi;
+       tid += (long long)gridDim.x * blockDim.x) {
+    int i = 1 + (int)(tid % g.nx);
+    long long r = tid / g.nx;
+    int j = 1 + (int)(r % g.ny);
+    int k = 1 + (int)(r / g.ny);
+    long long p = gidx(g, i, j, k);
+    if (mask != nullptr && mask[p] != 0) continue;
+    double f = FI(fln, tid, NS + 1) / dt;
+    sum = sum + f * f;
+    double v[3] = {FG(wa, p, NS + 11), FG(wa, p, NS + 5), FG(wa, p, NS + 6)};
+#pragma unroll
+    for (int q = 0; q < 3; q++) { vmin[q] = dmin_(vmin[q], v[q]); vmax[q] = dmax_(vmax[q], v[q]); }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sum = sum + __shfl_xor_sync(0xffffffffu, sum, o);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      vmin[q] = dmin_(vmin[q], __shfl_xor_sync(0xffffffffu, vmin[q], o));
+      vmax[q] = dmax_(vmax[q], __shfl_xor_sync(0xffffffffu, vmax[q], o));
+    }
+  }
+  __shared__ double sm[7][8];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    sm[0][wid] = sum;
+    for (int q = 0; q < 3; q++) { sm[1 + q][wid] = vmin[q]; sm[4 + q][wid] = vmax[q]; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    const int nw = (int)(blockDim.x >> 5), q = threadIdx.x;
+    double m = sm[q][0];
+    for (int wv = 1; wv < nw; wv++) m = q == 0 ? m + sm[q][wv] : (q < 4 ? dmin_(m, sm[q][wv]) : dmax_(m, sm[q][wv]));
+    if (q == 0) part[blockIdx.x] = m;
+    else if (q < 4) atomicMin(mm + q - 1, (unsigned long long)__double_as_longlong(m));
+    else atomicMax(mm + q - 1, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
 // ============================================================== launchers
 template <int NS>
 static int eval_aux_t(const DevCtx &c, cudaStream_t s, double *w, double *wa, int i0, int i1, int j0, int j1, int k0, int k1) {
@@ -431,6 +755,34 @@ int launch_bc_face(const DevCtx &c, cudaStream_t s, double *w, int ilat, int tag
   return STX_OK;
 }
 
+int launch_bc_face_thermo(const DevCtx &c, cudaStream_t s, double *w, double *wa, int ilat, int tag) {
+  int dir = (ilat - 1) / 2;
+  if (tag == 6 && dir != 1) return STX_OK;           // bcwall_cuf acts on the y sides only
+  long long n = (long long)(dir == 0 ? c.g.ny : c.g.nx) * (dir == 2 ? c.g.ny : c.g.nz);
+  switch (c.t.ns) {
+#define X(N) case N: k_bc_face_thermo<N><<<grid1d(n, 128), 128, 0, s>>>(c, w, wa, ilat, tag); break;
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_bc_nr(const DevCtx &c, cudaStream_t s, const double *wa, const double *w, double *fl, const double *winf,
+                 int ilat, int nr_type) {
+  int dir = (ilat - 1) / 2;
+  long long n = (long long)(dir == 0 ? c.g.ny : c.g.nx) * (dir == 2 ? c.g.ny : c.g.nz);
+  switch (c.t.ns) {
+#define X(N) case N: k_bc_nr<N><<<grid1d(n, 64), 64, 0, s>>>(c, wa, w, fl, winf, ilat, nr_type); break;
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
 int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt) {
   long long n = c.g.npi * (c.t.ns + 4);
   int nb = grid1d(n, 256);
@@ -471,6 +823,22 @@ int launch_compute_dt(const DevCtx &c, cudaStream_t s, const double *wa, const i
   if (nb > 148 * 8) nb = 148 * 8;
   switch (c.t.ns) {
 #define X(N) case N: k_compute_dt<N><<<nb, 256, 0, s>>>(c, wa, mask, out9); break;
+    STX_FOR_NS(X)
+#undef X
+    default: return STX_E_UNSUPPORTED;
+  }
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+int launch_residual_minmax(const DevCtx &c, cudaStream_t s, const double *fln, const double *wa, const int32_t *mask,
+                           double dt, double *part, unsigned long long *mm) {
+  // minima start at +inf (0x7ff0...), maxima at +0
+  static const unsigned long long init[6] = {0x7ff0000000000000ull, 0x7ff0000000000000ull, 0x7ff0000000000000ull,
+                                             0ull, 0ull, 0ull};
+  STX_CUDA_TRY(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  switch (c.t.ns) {
+#define X(N) case N: k_residual_minmax<N><<<STX_RES_BLOCKS, 256, 0, s>>>(c, fln, wa, mask, dt, part, mm); break;
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;

@@ -18,11 +18,15 @@
 #define STX_ROK4_MINB 4
 #endif
 
+// cg: a device-resident copy of c.  The right-hand side is one out-of-line
+// function that takes the context by reference; given the kernel parameter c,
+// every thread would keep its own local copy of the whole context (~0.9 KB),
+// given cg all threads read the one copy through L1.
 template <int NS>
 __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
-    k_rok4(DevCtx c, double *__restrict__ w, const double *__restrict__ wa,
-                                              const double *__restrict__ fl_sav, double dttry, double t0, double t1,
-                                              int simpler, unsigned int *counter) {
+    k_rok4(DevCtx c, const DevCtx *__restrict__ cg, double *__restrict__ w, const double *__restrict__ wa,
+           const double *__restrict__ fl_sav, double dttry, double t0, double t1, int simpler,
+           unsigned int *counter) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
   const double eps_Z = 5e-4;
@@ -40,13 +44,11 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
     long long p = gidx(g, i, j, k);
     double Z = FG(wa, p, NS + 12);
     if (!(Z > eps_Z && Z < 1.0 - eps_Z)) continue;
-    double VEC[NV], fls[NV];
+    double VEC[NV];
 #pragma unroll
-    for (int m = 0; m < NV; m++) {
-      VEC[m] = FG(w, p, m + 1);
-      fls[m] = (simpler == 1) ? FI(fl_sav, cell, m + 1) : 0.0;
-    }
-    rok4_cell<NS>(c, VEC, FG(wa, p, NS + 5), fls, dttry, t0, t1, simpler);
+    for (int m = 0; m < NV; m++) VEC[m] = FG(w, p, m + 1);
+    rok4_cell<NS>(*cg, VEC, FG(wa, p, NS + 5), simpler == 1 ? fl_sav + cell : nullptr, g.npi, dttry, t0, t1,
+                  simpler);
 #pragma unroll
     for (int m = 0; m < NV; m++) FG(w, p, m + 1) = VEC[m];
   }
@@ -55,13 +57,16 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
 // n independent adiabatic constant-pressure 0-D reactors, one thread each,
 // claimed from the work-stealing counter (reactors ignite at very different
 // times, so their step counts differ by orders of magnitude).  Y0 / Y are
-// (n, ns) with the reactor index fastest.
+// (n, ns) with the reactor index fastest.  cg: the device-resident context (the
+// right-hand side takes it by reference, see k_rok4); maxsteps: the step cap.
 template <int NS>
 __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
-    k_batch0d(DevCtx c, int n, const double *__restrict__ T0, const double *__restrict__ p0,
+    k_batch0d(const DevCtx *__restrict__ cg, int maxsteps, int n, const double *__restrict__ T0,
+              const double *__restrict__ p0,
               const double *__restrict__ Y0, double t_max, double dttry, double ign_factor, double end_factor,
               double *__restrict__ Y, double *__restrict__ T, double *__restrict__ t_ign, double *__restrict__ t_end,
               int *__restrict__ nsteps, unsigned int *counter) {
+  const DevCtx &c = *cg;
   for (;;) {
     long long r = claim(counter);
     if (r >= n) break;
@@ -73,7 +78,7 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
 #pragma unroll 1
     for (int k = 0; k < NS; k++) h = h + VEC[k] * species_poly_int(c.t, c.t.cpi, T0r, k + 1);
     Rok4ConstP<NS> f{c, h, p0[r], T0r, ign_factor, end_factor, -1.0, 0.0, T0r, 0};
-    rok4_core<NS>(c, f, VEC, T0r, nullptr, dttry, 0.0, t_max, 0);
+    rok4_core<NS>(c, f, VEC, T0r, nullptr, 0, dttry, 0.0, t_max, 0, maxsteps);
 #pragma unroll
     for (int k = 0; k < NS; k++) Y[(long long)k * n + r] = VEC[k];
     T[r] = f.T_final;
@@ -341,13 +346,13 @@ int chem_ctas_limit(int ns) {
 }
 
 template <int NS>
-static int rok4_t(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
-                  double t0, double t1, int simpler, unsigned int *counter) {
+static int rok4_t(const DevCtx &c, const DevCtx *cg, cudaStream_t s, double *w, const double *wa, const double *fl_sav,
+                  double dttry, double t0, double t1, int simpler, unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
   int nb = persistent_blocks((const void *)k_rok4<NS>, chem_block(NS), c.p.chem_ctas_per_sm);
   long long need = (c.g.npi + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
-  k_rok4<NS><<<nb, chem_block(NS), 0, s>>>(c, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
+  k_rok4<NS><<<nb, chem_block(NS), 0, s>>>(c, cg, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
@@ -364,10 +369,10 @@ static int ros_t(const DevCtx &c, cudaStream_t s, double *w, double *wa, double 
   return STX_OK;
 }
 
-int launch_rok4(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
-                double t0, double t1, int simpler, unsigned int *counter) {
+int launch_rok4(const DevCtx &c, const DevCtx *cg, cudaStream_t s, double *w, const double *wa, const double *fl_sav,
+                double dttry, double t0, double t1, int simpler, unsigned int *counter) {
   switch (c.t.ns) {
-#define X(N) case N: return rok4_t<N>(c, s, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
+#define X(N) case N: return rok4_t<N>(c, cg, s, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;
@@ -375,7 +380,8 @@ int launch_rok4(const DevCtx &c, cudaStream_t s, double *w, const double *wa, co
 }
 
 template <int NS>
-static int batch0d_t(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
+static int batch0d_t(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int n, const double *T0, const double *p0,
+                     const double *Y0,
                      double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
                      double *t_end, int *nsteps, unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
@@ -383,17 +389,17 @@ static int batch0d_t(const DevCtx &c, cudaStream_t s, int n, const double *T0, c
   long long need = ((long long)n + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
   if (c.p.batch_ctas_max > 0 && nb > c.p.batch_ctas_max) nb = c.p.batch_ctas_max;
-  k_batch0d<NS><<<nb, chem_block(NS), 0, s>>>(c, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps,
-                                              counter);
+  k_batch0d<NS><<<nb, chem_block(NS), 0, s>>>(cg, c.p.ros_maxsteps, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T,
+                                              t_ign, t_end, nsteps, counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
 
-int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
-                   double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
-                   double *t_end, int *nsteps, unsigned int *counter) {
+int launch_batch0d(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int n, const double *T0, const double *p0,
+                   const double *Y0, double t_max, double dttry, double ign, double endf, double *Y, double *T,
+                   double *t_ign, double *t_end, int *nsteps, unsigned int *counter) {
   switch (c.t.ns) {
-#define X(N) case N: return batch0d_t<N>(c, s, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps, counter);
+#define X(N) case N: return batch0d_t<N>(c, cg, s, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T, t_ign, t_end, nsteps, counter);
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;

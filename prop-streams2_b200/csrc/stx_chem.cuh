@@ -318,9 +318,21 @@ static __device__ void inv_matrix_k(double *a, int d) {
 //   f.accept(y, time, T_iter, time_end) after an accepted step: updates the
 //                                       temperature guess, may move time_end;
 //   f.done(time, T_iter, steps)         at the end: time reached, last T, steps.
+// fls (simpler == 1 only) is the cell's saved residual fl_sav, component m at
+// fls[m * fstride]; maxsteps caps the steps (ros_maxsteps).
+//
+// Per-thread working set, kept small because it lives in local memory for
+// every resident thread: V (Krylov basis), inv, the stage vectors Ks and one
+// 3 x NV scratch that serves the Arnoldi temporaries (jac, wl), the stage
+// temporaries (ys, F, GK) and the new state.  The right-hand side at the
+// start of a step, f(VEC), is formed once: the Arnoldi iteration uses it (less
+// fl_sav: rhs_sav), and the first stage, whose state is VEC itself and whose
+// temperature guess is the same, reuses it with the operations the reference
+// applies to a fresh evaluation (f(VEC) + 0 - fl_sav), so the result is the
+// same bit for bit with one right-hand side fewer per step.
 template <int NV, class F>
-__device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, const double *fls, double dttry,
-                          double time_start, double time_end, int simpler) {
+__device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, const double *fls, long long fstride,
+                          double dttry, double time_start, double time_end, int simpler, int maxsteps) {
   const double gam = 0.572816062482135;
   const double a21 = 0.432364435748567, a31 = -0.514211316876170, a32 = 1.382271144617360;
   const double a41 = -0.514211316876170, a42 = 1.382271144617360, a43 = 0.0;
@@ -333,8 +345,12 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
   const double bsv[4] = {bs1, bs2, bs3, bs4}, btv[4] = {bt1, bt2, bt3, bt4};
   double V[NV * (STX_MMAX + 1)];
   double inv[STX_MMAX * STX_MMAX];
-  double Ks[NV * STX_NSTAGE];
-  double rhs_sav[NV];
+  double Ks[NV * STX_NSTAGE];                // Ks[0..NV) holds f(VEC) until stage 1 replaces it
+  double S0[NV], S1[NV], S2[NV];             // scratch: jac / wl, then ys / F / GK, then the new state
+  double *raw = Ks;
+  auto fsav = [&](int m) -> double { return fls[(long long)m * fstride]; };
+  // rhs_sav of the reference: f(VEC), less fl_sav with the simpler splitting
+  auto rhs_sav = [&](int m) -> double { return simpler == 1 ? raw[m] - fsav(m) : raw[m]; };
   int mA = 0;
 #pragma unroll
   for (int q = 0; q < STX_MMAX * STX_MMAX; q++) inv[q] = 0.0;
@@ -354,21 +370,24 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
 #pragma unroll
       for (int q = 0; q < NV * (STX_MMAX + 1); q++) V[q] = 0.0;
       mA = 0;
-      f.rhs(VEC, T_iter, rhs_sav);
-      if (simpler == 1)
-        for (int m = 0; m < NV; m++) rhs_sav[m] = rhs_sav[m] - fls[m];
-      double nrm = norm2v<NV>(rhs_sav);
-      for (int m = 0; m < NV; m++) V[m] = rhs_sav[m] / nrm;
+      f.rhs(VEC, T_iter, raw);
+      double nrm;
+      {
+        double sq = 0.0;
+        for (int m = 0; m < NV; m++) { const double r = rhs_sav(m); sq = sq + r * r; }
+        nrm = sqrt(sq);
+      }
+      for (int m = 0; m < NV; m++) V[m] = rhs_sav(m) / nrm;
       // the outer loops stay rolled (unroll 1): unrolled, the Krylov algebra
       // is straight-line code far larger than the instruction cache
 #pragma unroll 1
       for (int kk = 1; kk <= STX_MMAX; kk++) {
-        double jac[NV], wl[NV];
+        double *jac = S0, *wl = S1;
         for (int m = 0; m < NV; m++) wl[m] = VEC[m] + (eps * V[(kk - 1) * NV + m]);
         f.rhs(wl, T_iter, jac);
         if (simpler == 1)
-          for (int m = 0; m < NV; m++) jac[m] = jac[m] - fls[m];
-        for (int m = 0; m < NV; m++) jac[m] = (jac[m] - rhs_sav[m]) / eps;
+          for (int m = 0; m < NV; m++) jac[m] = jac[m] - fsav(m);
+        for (int m = 0; m < NV; m++) jac[m] = (jac[m] - rhs_sav(m)) / eps;
 #pragma unroll 1
         for (int jj = 1; jj <= kk; jj++) {
           double dot = 0.0;
@@ -384,7 +403,7 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
         for (int ll = 1; ll <= STX_MMAX; ll++) {
           double s = 0.0;
           if (ll <= kk)
-            for (int m = 0; m < NV; m++) s = s + V[(ll - 1) * NV + m] * rhs_sav[m];
+            for (int m = 0; m < NV; m++) s = s + V[(ll - 1) * NV + m] * rhs_sav(m);
           prj[ll - 1] = s;
         }
 #pragma unroll 1
@@ -417,25 +436,29 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
     // stage; the sums are regrouped (rounding-level difference).
 #pragma unroll 1
     for (int ii = 1; ii <= STX_NSTAGE; ii++) {
-      double ys[NV], F[NV], GK[NV];
-      for (int m = 0; m < NV; m++) ys[m] = VEC[m];
+      double *ys = S0, *Fv = S1, *GK = S2;
+      if (ii == 1) {
+        for (int m = 0; m < NV; m++) Fv[m] = raw[m];            // f(VEC), formed for the Arnoldi iteration
+      } else {
+        for (int m = 0; m < NV; m++) ys[m] = VEC[m];
 #pragma unroll 1
-      for (int jj = 1; jj <= ii - 1; jj++)
-        for (int m = 0; m < NV; m++) ys[m] = ys[m] + dt * alpha[ii - 1][jj - 1] * Ks[(jj - 1) * NV + m];
-      f.rhs(ys, T_iter, F);
+        for (int jj = 1; jj <= ii - 1; jj++)
+          for (int m = 0; m < NV; m++) ys[m] = ys[m] + dt * alpha[ii - 1][jj - 1] * Ks[(jj - 1) * NV + m];
+        f.rhs(ys, T_iter, Fv);
+      }
       for (int m = 0; m < NV; m++) GK[m] = 0.0;
 #pragma unroll 1
       for (int jj = 1; jj <= ii - 1; jj++)
         for (int m = 0; m < NV; m++) GK[m] = GK[m] + gmc[ii - 1][jj - 1] / gam * Ks[(jj - 1) * NV + m];
-      for (int m = 0; m < NV; m++) F[m] = F[m] + GK[m];
+      for (int m = 0; m < NV; m++) Fv[m] = Fv[m] + GK[m];
       if (simpler == 1)
-        for (int m = 0; m < NV; m++) F[m] = F[m] - fls[m];
+        for (int m = 0; m < NV; m++) Fv[m] = Fv[m] - fsav(m);
       double pf[STX_MMAX];
 #pragma unroll
       for (int q = 0; q < STX_MMAX; q++) {
         double s = 0.0;
         if (q < mA)
-          for (int jj = 0; jj < NV; jj++) s = s + V[q * NV + jj] * F[jj];
+          for (int jj = 0; jj < NV; jj++) s = s + V[q * NV + jj] * Fv[jj];
         pf[q] = s;
       }
 #pragma unroll 1
@@ -451,10 +474,12 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
           for (int jj = 1; jj < STX_MMAX; jj++) a = a + vb[jj] * ((jj == kk ? 1.0 : 0.0) - inv[kk * STX_MMAX + jj]);
           s = s + a * pf[kk];
         }
-        Ks[(ii - 1) * NV + ll] = F[ll] - s - GK[ll];
+        Ks[(ii - 1) * NV + ll] = Fv[ll] - s - GK[ll];
       }
     }
-    double ys[NV], errv[NV];
+    // the new state and its error norm (the norm's sum in component order)
+    double *ys = S0;
+    double esq = 0.0;
     for (int ll = 0; ll < NV; ll++) {
       double a = VEC[ll], b = VEC[ll];
       for (int ii = 0; ii < STX_NSTAGE; ii++) {
@@ -462,9 +487,10 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
         b = b + dt * btv[ii] * Ks[ii * NV + ll];
       }
       ys[ll] = a;
-      errv[ll] = (b - a) / ((1.0e-4) * a + 1.0e-8);
+      const double ev = (b - a) / ((1.0e-4) * a + 1.0e-8);
+      esq = esq + ev * ev;
     }
-    double errmax = norm2v<NV>(errv);
+    double errmax = sqrt(esq);
     double fac = 0.625 * pow(errn, 0.1) / pow(errmax, 0.175);
     double dtnext = dt * dmin_(5.0, dmax_(0.2, fac));
     if (errmax < 1.0) {
@@ -474,7 +500,7 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
     }
     dt = dtnext;
     errn = errmax;
-    if (it > c.p.ros_maxsteps) { set_status(c.p, STX_ST_ROS_STEPS_CAP); break; }
+    if (it > maxsteps) { set_status(c.p, STX_ST_ROS_STEPS_CAP); break; }
   }
   f.done(time, T_iter, it);
 }
@@ -560,12 +586,13 @@ struct Rok4ConstP {
   }
 };
 
-// One ROK4 flow cell.
+// One ROK4 flow cell; fls: the cell's fl_sav components at stride fstride (simpler == 1).
 template <int NS, bool KCF = false>
-__device__ __forceinline__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const double *fls, double dttry,
-                                          double time_start, double time_end, int simpler) {
+__device__ __forceinline__ void rok4_cell(const DevCtx &c, double *VEC, double T_iter, const double *fls,
+                                          long long fstride, double dttry, double time_start, double time_end,
+                                          int simpler) {
   Rok4Flow<NS, KCF> f{c};
-  rok4_core<NS + 4>(c, f, VEC, T_iter, fls, dttry, time_start, time_end, simpler);
+  rok4_core<NS + 4>(c, f, VEC, T_iter, fls, fstride, dttry, time_start, time_end, simpler, c.p.ros_maxsteps);
 }
 
 // claim the next cell: warp-aggregated atomicAdd over the currently active lanes

@@ -16,7 +16,9 @@
 #define STX_SPW (4 * STX_SPR)   // sparse row: reactants, products, union (2 STX_SPR)
 
 // species counts compiled into the library
+#ifndef STX_FOR_NS
 #define STX_FOR_NS(X) X(9) X(11) X(13) X(14) X(53)
+#endif
 
 // CTA sizes of the kernels that keep NS-long per-thread rows (chemistry) or
 // (NS+4)-long per-face rows (the x sweeps) in shared memory: smaller CTAs for
@@ -88,6 +90,8 @@ struct DevPar {
   // most CTAs of a batched-reactor launch (0: no cap), so that several
   // concurrent launches leave the SMs room for other work
   int batch_ctas_max;
+  // wall temperature of the isothermal-wall ghost fill (bc tag 6)
+  double T_wall;
 };
 
 struct DevCtx {

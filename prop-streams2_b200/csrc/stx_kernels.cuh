@@ -7,12 +7,21 @@ int launch_eval_aux2(const DevCtx &c, cudaStream_t s, double *wa);
 int launch_bcextr_var(const DevCtx &c, cudaStream_t s, double *v);
 int launch_bcswap(const DevCtx &c, cudaStream_t s, double *f, int nvar, const int *periodic);
 int launch_bc_face(const DevCtx &c, cudaStream_t s, double *w, int ilat, int tag, const double *winf);
+// ghost fills that need the thermodynamics and w_aux (bc tags 4 and 6)
+int launch_bc_face_thermo(const DevCtx &c, cudaStream_t s, double *w, double *wa, int ilat, int tag);
+// characteristic boundary treatment of face ilat (bc_nr_lat_*), added to fl
+int launch_bc_nr(const DevCtx &c, cudaStream_t s, const double *wa, const double *w, double *fl, const double *winf,
+                 int ilat, int nr_type);
 int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt);
 int launch_update_flux(const DevCtx &c, cudaStream_t s, const double *fl, double *fln, const double *fl_sav, double gamdt);
 int launch_copy(const DevCtx &c, cudaStream_t s, const double *a, double *b);
 int launch_update_field(const DevCtx &c, cudaStream_t s, double *w, const double *fl, double *fln, const double *fl_sav,
                         const int32_t *mask, double gamdt, int fused);
 int launch_compute_dt(const DevCtx &c, cudaStream_t s, const double *wa, const int32_t *mask, unsigned long long *out9);
+// compute_residual + rho/T/p extrema: STX_RES_BLOCKS partial sums in part, 6 extrema in mm
+#define STX_RES_BLOCKS 296
+int launch_residual_minmax(const DevCtx &c, cudaStream_t s, const double *fln, const double *wa, const int32_t *mask,
+                           double dt, double *part, unsigned long long *mm);
 
 // Scratch of the listed WENO faces (stx_euler.cu): a counter, the ids of the
 // faces the Ducros sensor marks, and their fluxes by face id (nv x cap).
@@ -36,14 +45,16 @@ int launch_visflx_reduced(const DevCtx &c, cudaStream_t s, const double *wa, dou
 
 // occupancy limit (CTAs per SM) of the ROK4 cell kernel for ns species
 int chem_ctas_limit(int ns);
-int launch_rok4(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry,
-                double t0, double t1, int simpler, unsigned int *counter);
+// cg: the device-resident copy of c (stx_ctx::dctx_d)
+int launch_rok4(const DevCtx &c, const DevCtx *cg, cudaStream_t s, double *w, const double *wa, const double *fl_sav,
+                double dttry, double t0, double t1, int simpler, unsigned int *counter);
 int launch_rosenbrock(const DevCtx &c, cudaStream_t s, double *w, double *wa, double dttry, double t0, double t1,
                       unsigned int *counter);
 int launch_chem_explicit(const DevCtx &c, cudaStream_t s, double *w, double *wa, double *fl);
-int launch_batch0d(const DevCtx &c, cudaStream_t s, int n, const double *T0, const double *p0, const double *Y0,
-                   double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
-                   double *t_end, int *nsteps, unsigned int *counter);
+// cg: the device-resident context (its ros_maxsteps is not read: c's is the cap)
+int launch_batch0d(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int n, const double *T0, const double *p0,
+                   const double *Y0, double t_max, double dttry, double ign, double endf, double *Y, double *T,
+                   double *t_ign, double *t_end, int *nsteps, unsigned int *counter);
 // once per device and species count: shared-memory split of the persistent
 // warp-per-reactor kernel
 int launch_batch0d_setup(int ns);

@@ -39,13 +39,11 @@ __global__ void __launch_bounds__(128) k_rok4_noalloc(DevCtx c, double *__restri
     long long p = gidx(g, i, j, k);
     double Z = FG(wa, p, NS + 12);
     if (!(Z > eps_Z && Z < 1.0 - eps_Z)) continue;
-    double VEC[NV], fls[NV];
+    double VEC[NV];
 #pragma unroll
-    for (int m = 0; m < NV; m++) {
-      VEC[m] = FG(w, p, m + 1);
-      fls[m] = (simpler == 1) ? FI(fl_sav, cell, m + 1) : 0.0;
-    }
-    rok4_cell<NS, true>(c, VEC, FG(wa, p, NS + 5), fls, dttry, t0, t1, simpler);
+    for (int m = 0; m < NV; m++) VEC[m] = FG(w, p, m + 1);
+    rok4_cell<NS, true>(c, VEC, FG(wa, p, NS + 5), simpler == 1 ? fl_sav + cell : nullptr, g.npi, dttry, t0, t1,
+                        simpler);
 #pragma unroll
     for (int m = 0; m < NV; m++) FG(w, p, m + 1) = VEC[m];
   }
@@ -54,14 +52,16 @@ __global__ void __launch_bounds__(128) k_rok4_noalloc(DevCtx c, double *__restri
 namespace {
 
 // Device address of g_noalloc_counter, looked up once per device with that
-// device current (the host-side symbol is not a device address).
+// device current (the host-side symbol is not a device address).  The cache
+// holds for the life of the device's primary context: after cudaDeviceReset the
+// library's module is loaded anew and the cached address is stale, so a caller
+// that resets a device must not call this entry point on it again.
 std::mutex g_mu;
 unsigned int *g_addr[64];
 bool g_ready[64];
 
-int counter_address(unsigned int **out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return STX_E_CUDA;
+int counter_address(int dev, unsigned int **out) {
+  if (dev < 0 || dev >= 64) return STX_E_CUDA;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_ready[dev]) {
     void *p = nullptr;
@@ -73,11 +73,29 @@ int counter_address(unsigned int **out) {
   return STX_OK;
 }
 
+// The kernel keeps its per-thread working set (Krylov basis, stage vectors, the
+// frame of the out-of-line right-hand side) in local memory.  The driver backs
+// local memory with a reservation of cudaLimitStackSize bytes for every thread
+// the device can hold, and grows it -- a device allocation of (frame x resident
+// threads), about 1 GB for 9 species on a B200 -- when a launch needs more than
+// the current limit.  That growth would break this entry point's promise, so a
+// launch that would trigger it is refused with STX_E_LOCAL_MEM instead; the
+// caller raises the limit once at initialisation (cudaDeviceSetLimit).
 template <int NS>
-int launch(const DevCtx &c, cudaStream_t s, double *w, const double *wa, const double *fl_sav, double dttry, double t0,
-           double t1, int simpler, unsigned int *counter) {
-  int dev = 0, nsm = 148, per = 1;
-  cudaGetDevice(&dev);
+int local_memory_ok() {
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, (const void *)k_rok4_noalloc<NS>) != cudaSuccess) return STX_E_CUDA;
+  size_t lim = 0;
+  if (cudaDeviceGetLimit(&lim, cudaLimitStackSize) != cudaSuccess) return STX_E_CUDA;
+  return fa.localSizeBytes <= lim ? STX_OK : STX_E_LOCAL_MEM;
+}
+
+template <int NS>
+int launch(const DevCtx &c, cudaStream_t s, int dev, double *w, const double *wa, const double *fl_sav, double dttry,
+           double t0, double t1, int simpler, unsigned int *counter) {
+  int rc = local_memory_ok<NS>();
+  if (rc != STX_OK) return rc;
+  int nsm = 148, per = 1;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)k_rok4_noalloc<NS>, 128, 0);
   long long nb = (long long)nsm * (per < 1 ? 1 : per);
@@ -126,12 +144,19 @@ extern "C" int stx_rosenbrock_krylov_noalloc(const stx_params *par, const stx_ta
   p.ros_maxsteps = par->ros_maxsteps;
   p.ros_eps = par->ros_eps;
   p.status = status;
-  unsigned int *counter = nullptr;
-  int rc = counter_address(&counter);
-  if (rc != STX_OK) return rc;
   cudaStream_t s = (cudaStream_t)stream;
+  // the scratch and the launch belong to the current device; a stream of
+  // another device would pair it with the wrong device's counter
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return STX_E_CUDA;
+  int sdev = dev;
+  if (s != nullptr && cudaStreamGetDevice(s, &sdev) != cudaSuccess) return STX_E_CUDA;
+  if (sdev != dev) return STX_E_INVALID;
+  unsigned int *counter = nullptr;
+  int rc = counter_address(dev, &counter);
+  if (rc != STX_OK) return rc;
   switch (t.ns) {
-#define X(N) case N: return launch<N>(c, s, w, w_aux, fl_sav, dttry, time_start, time_end, simpler, counter);
+#define X(N) case N: return launch<N>(c, s, dev, w, w_aux, fl_sav, dttry, time_start, time_end, simpler, counter);
     STX_FOR_NS(X)
 #undef X
     default: return STX_E_UNSUPPORTED;

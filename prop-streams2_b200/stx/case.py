@@ -26,6 +26,10 @@ from . import mech as M
 from .native import StxGrid, StxParams, StxTables
 
 TOL_ITER = 1e-9        # src/parameters.F90:49
+# ghost-fill tags of update_ghost on this path (multideal_gpu.F90:1176-1233): 0 periodic,
+# 1 free stream, 2 extrapolation, 4 subsonic extrapolation at p0, 5 symmetry,
+# 6 isothermal wall, 7 open outflow, 8 adiabatic wall
+BC_TAGS = (0, 1, 2, 4, 5, 6, 7, 8)
 TOL_ITER_NR = 1e-12    # src/parameters.F90:50
 
 # deriv coefficients (grid.F90:135-182)
@@ -95,10 +99,12 @@ class Case:
                 self.bctags[2 * d] = self.bctags[2 * d + 1] = 0
                 self.periodic[d] = True
         for t in self.bctags:
-            if t not in (0, 1, 2, 8):
-                raise ValueError(f"bc tag {t} is outside the supported hot path (0,1,2,8)")
-        if any(self.bctags_nr):
-            raise ValueError("non-reflecting boundary treatment (bc *_nr > 0) is not on this path")
+            if t not in BC_TAGS:
+                raise ValueError(f"bc tag {t} is outside the supported path {sorted(BC_TAGS)} "
+                                 "(9 laminar-profile inflow, 10 recycling, 26/28 jets, 46/56 special walls are not)")
+        for t in self.bctags_nr:
+            if t not in (0, 1, 2, 3, 6):
+                raise ValueError(f"bc *_nr = {t}: the characteristic treatment takes 0, 1, 2, 3 or 6")
         # --- grid (uniform only)
         gtype = cfg.get("grid", "grid_type", kind=int)
         if gtype != 2:
@@ -175,9 +181,15 @@ class Case:
         if abs(self.u0) < TOL_ITER:
             self.u0 = self.c0
         self.eps_sensor = self.u0 ** 2
-        # --- bc_preproc (multideal.F90:5671-5718)
+        # --- bc_preproc (multideal.F90:5671-5718): a face with a characteristic
+        # treatment leaves its boundary cells out of the convective flux
+        # divergence (bc_nr supplies their convective term)
         self.force_zero_flux = [0] * 6
         self.eul = [1, self.nx, 1, self.ny, 1, self.nz]
+        for ilat in range(6):
+            if self.bctags_nr[ilat] != 0:
+                self.eul[ilat] += 1 if ilat % 2 == 0 else -1
+        self.T_wall = cfg.get("flow", "T_wall", 0.0) if cfg.has_key("flow", "T_wall") else self.t0
         # --- fields
         self.nxg, self.nyg, self.nzg = self.nx + 2 * self.ng, self.ny + 2 * self.ng, self.nz + 2 * self.ng
         self._keep = []
@@ -198,6 +210,8 @@ class Case:
             self._init_reactive_tube()
         elif self.flow_init in (-1,):
             pass
+        elif self.flow_init == 10:
+            pass    # init_premix: the profile comes from premix.dat (init_premix below)
         elif self.flow_init == 100:
             pass    # caller-provided field (synthetic cases)
         else:
@@ -264,6 +278,26 @@ class Case:
             if x[i + ng - 1] >= 0.5 * x[self.nx + ng - 1]:
                 self.w[:, ng:ng + self.nz, ng:ng + self.ny, i + ng - 1] = wt[:, None, None]
 
+    def init_premix(self, u, T, Y):
+        """init_premix (multideal.F90:5534-5606): the 1-D profile of premix.dat (per
+        cell i: u, T, Y_1..Y_ns) on every (j, k) line, at the reference pressure.
+        As in the reference, the mixture gas constant and rho*Y_k use the file's
+        mass fractions as they are, while the internal energy is evaluated with
+        |Y_k| < 1e-25 set to zero."""
+        u, T = np.asarray(u, float)[: self.nx], np.asarray(T, float)[: self.nx]
+        Y = np.asarray(Y, float)[:, : self.nx]
+        rm = np.einsum("k,kx->x", self.tb.rgas, Y)
+        Yc = np.where(np.abs(Y) < 1e-25, 0.0, Y)
+        rho = self.p0 / rm / T
+        e = mixture_e_field(self.tb, T, Yc)
+        ng, ns = self.ng, self.ns
+        sl = (slice(ng, ng + self.nz), slice(ng, ng + self.ny), slice(ng, ng + self.nx))
+        self.w[(slice(0, ns),) + sl] = (rho[None, :] * Y)[:, None, None, :]
+        self.w[(ns,) + sl] = (rho * u)[None, None, :]
+        self.w[(ns + 1,) + sl] = 0.0
+        self.w[(ns + 2,) + sl] = 0.0
+        self.w[(ns + 3,) + sl] = (rho * (e + 0.5 * u * u))[None, None, :]
+
     def set_interior(self, rho, u, v, w, T, Y):
         """Set the interior from primitive fields of shape (nz, ny, nx) (Y: (ns, nz, ny, nx))."""
         ng, ns = self.ng, self.ns
@@ -304,6 +338,7 @@ class Case:
             p.rhork[q] = self.rhork[q]
             p.gamrk[q] = self.gamrk[q]
         p.winf = self._p(self.winf)
+        p.T_wall = self.T_wall
         return p
 
     def tables_struct(self) -> StxTables:
@@ -380,10 +415,20 @@ def mixture_e_field(tb: M.Tables, T: np.ndarray, Y: np.ndarray) -> np.ndarray:
     return e
 
 
+def read_premix(path: str, ns: int):
+    """The reference's premix.dat (one line per cell: x, u, T, Y_1..Y_ns) as arrays
+    x, u, T (n) and Y (ns, n)."""
+    a = np.loadtxt(path, ndmin=2)
+    if a.shape[1] != 3 + ns:
+        raise ValueError(f"{path}: {a.shape[1]} columns, expected {3 + ns}")
+    return a[:, 0], a[:, 1], a[:, 2], a[:, 3:].T.copy()
+
+
 def default_ini(nx, ny, nz, L=(1.0, 1.0, 1.0), bc=(0, 0, 0, 0, 0, 0), t0=1000.0, p0=101325.0,
                 Y=None, ns=9, chemistry=2, rosenbrock_version=2, splitting=2, weno_version=1,
                 sensor_threshold=0.1, sensor_type=1, nkeep=1, ep_order=6, flux_splitting=0,
-                cfl=0.5, flow_init=100) -> Config:
+                cfl=0.5, flow_init=100, weno_scheme=3, ng=3, bc_nr=(0, 0, 0, 0, 0, 0),
+                T_wall=None) -> Config:
     """A Config with the keys the solver reads, for synthetic cases."""
     cfg = Config()
     cfg.set("ref_state", "t0", t0); cfg.set("ref_state", "p0", p0); cfg.set("ref_state", "u0", 0.0)
@@ -392,16 +437,18 @@ def default_ini(nx, ny, nz, L=(1.0, 1.0, 1.0), bc=(0, 0, 0, 0, 0, 0), t0=1000.0,
             cfg.set("ref_state", f"init_Y_{k + 1:02d}", repr(float(y)))
     for a, n, l in zip("xyz", (nx, ny, nz), L):
         cfg.set("grid", f"n{a}max", n); cfg.set("grid", f"domain_size_{a}", repr(float(l)))
-    cfg.set("grid", "ng", 3); cfg.set("grid", "metrics_order", ep_order); cfg.set("grid", "grid_type", 2)
-    for k, v in zip(["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"], bc):
-        cfg.set("bc", k, v); cfg.set("bc", k + "_nr", 0)
+    cfg.set("grid", "ng", ng); cfg.set("grid", "metrics_order", ep_order); cfg.set("grid", "grid_type", 2)
+    for k, v, vn in zip(["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"], bc, bc_nr):
+        cfg.set("bc", k, v); cfg.set("bc", k + "_nr", vn)
     cfg.set("controls", "cfl", cfl); cfg.set("controls", "num_iter", 1); cfg.set("controls", "iter_dt_recompute", 1)
     for k, v in dict(ep_order=ep_order, nkeep=nkeep, visc_order=ep_order, conservative_viscous=1,
-                     weno_scheme=3, weno_version=weno_version, flux_splitting=flux_splitting,
+                     weno_scheme=weno_scheme, weno_version=weno_version, flux_splitting=flux_splitting,
                      sensor_threshold=sensor_threshold, sensor_type=sensor_type, rk_type=1,
                      ros_dttry=1e-9, ros_eps=1e-8, ros_maxsteps=10000, ros_maxtry=40,
                      operator_splitting=splitting, rosenbrock_version=rosenbrock_version).items():
         cfg.set("numerics", k, v)
     cfg.set("flow", "flow_init", flow_init)
+    if T_wall is not None:
+        cfg.set("flow", "T_wall", T_wall)
     cfg.set("fluid", "use_cantera", 1); cfg.set("fluid", "enable_chemistry", chemistry)
     return cfg

@@ -195,6 +195,19 @@ def tube_case(nx: int, ny: int = 1, tables: M.Tables = None):
     return CS.Case(cfg, tables)
 
 
+def config1_case(nx: int = 2400, cfl: float = 0.5, tables: M.Tables = None):
+    """The 1-D reactive shock tube on nx cells over 0.12 m with a CFL-driven step
+    (the reference's example, examples/reactive_shock_tube, runs 400 cells at a
+    fixed dt of 2e-8 s): reflecting wall at x = 0, extrapolation at x = 0.12 m,
+    H2:O2:Ar = 2:1:7 with the example's 9-species, 18-reaction mechanism, the
+    example's initial step at 0.06 m (left rho = 0.072, p = 7173 Pa, u = 0; right
+    rho = 0.18075, p = 35594 Pa, u = -487.34 m/s), WENO5 on every face,
+    Strang + ROK4."""
+    c = tube_case(nx, tables=tables)
+    c.cfl = cfl
+    return c
+
+
 def flame_case(nx: int, phi: float = 0.6, Tu: float = 298.0, tables: M.Tables = None, L: float = 0.03,
                delta: float = 3e-4, mech_name: str = "flame_11sp"):
     """A 1-D laminar premixed H2/air flame on nx cells of an L-long domain: the
@@ -250,6 +263,67 @@ def flame_case(nx: int, phi: float = 0.6, Tu: float = 298.0, tables: M.Tables = 
     c.set_interior(rho.reshape(sh), u.reshape(sh), np.zeros(sh), np.zeros(sh), T.reshape(sh),
                    Y.reshape((ns,) + sh))
     c.flame = dict(phi=phi, Tu=Tu, Tb=Tb, Yu=Yu, Yb=Yb)
+    return c
+
+
+# The laminar premixed flame's inputs (examples/laminar_premix_flame/multideal.ini):
+# 11-species, 21-reaction H2/O2 mechanism with Ar/He/N2, 2000 cells over 3 cm,
+# inflow (bc 1) at xmin and extrapolation at xmax, WENO5-Z on every face
+# (threshold -0.2) with KEEP(2), "simpler" splitting with ROK4, fixed dt 1e-8 s;
+# the initial profile is premix.dat (flow_init 10).
+FLAME_INI = {
+    "ref_state": {"t0": "298.", "p0": "101325.0", "u0": "0.9139672490375892",
+                  "init_Y_01": "0.0173109321627845", "init_Y_02": "0.", "init_Y_03": "0.2289662728773070",
+                  "init_Y_04": "0.", "init_Y_05": "0.", "init_Y_06": "0.", "init_Y_07": "0.", "init_Y_08": "0.",
+                  "init_Y_09": "0.", "init_Y_10": "0.", "init_Y_11": "0.7537227949599082"},
+    "grid": {"domain_size_x": "0.03", "domain_size_y": "1.", "domain_size_z": "1.", "nxmax": "2000", "nymax": "1",
+             "nzmax": "1", "ng": "3", "metrics_order": "6", "grid_type": "2"},
+    "bc": {"xmin": "1", "xmax": "2", "ymin": "0", "ymax": "0", "zmin": "0", "zmax": "0", "xmin_nr": "0",
+           "xmax_nr": "0", "ymin_nr": "0", "ymax_nr": "0", "zmin_nr": "0", "zmax_nr": "0"},
+    "controls": {"cfl": "-1E-8", "iter_dt_recompute": "1", "num_iter": "100000"},
+    "numerics": {"ep_order": "6", "nkeep": "2", "visc_order": "6", "conservative_viscous": "1", "weno_scheme": "3",
+                 "weno_version": "1", "flux_splitting": "0", "sensor_threshold": "-0.2", "sensor_type": "0",
+                 "rk_type": "1", "ros_dttry": "1.e-9", "ros_eps": "1.e-8", "ros_maxsteps": "10000",
+                 "ros_maxtry": "40", "operator_splitting": "1", "rosenbrock_version": "2"},
+    "flow": {"flow_init": "10"},
+    "fluid": {"use_cantera": "1", "enable_chemistry": "2", "t_min_tab": "200.", "t_max_tab": "20000.",
+              "dt_tab": "1."},
+}
+
+
+def premix_profile():
+    """The reference flame's initial profile (premix.dat of examples/laminar_premix_flame):
+    x, u, T (2000 cells) and Y (11, 2000)."""
+    d = np.load(os.path.join(DATA, "premix_flame_11sp.npz"))
+    return d["x"], d["u"], d["T"], d["Y"]
+
+
+def premix_flame_case(nx: int = 2000, tables: M.Tables = None, visc_scale: float = 1.0, lam_scale: float = 1.0,
+                      diff_scale: float = 1.0):
+    """The reference's laminar premixed flame run (examples/laminar_premix_flame):
+    its multideal.ini and its premix.dat profile (the first nx cells of it when
+    nx < 2000, with the domain shortened to keep the spacing).  visc_scale,
+    lam_scale and diff_scale multiply the species viscosity, conductivity and
+    binary-diffusion tables (sensitivity knobs for the transport tables, which
+    come from the project's kinetic-theory generator instead of Cantera)."""
+    cfg = CS.Config()
+    for sec, kv in FLAME_INI.items():
+        for k, v in kv.items():
+            cfg.set(sec, k, v)
+    if nx != 2000:
+        cfg.set("grid", "nxmax", nx)
+        cfg.set("grid", "domain_size_x", repr(0.03 * (nx - 1) / 1999.0))
+    if tables is None:
+        tables = M.build_tables(mechanism("flame_11sp"), 101325.0, 200.0, 20000.0, 1.0)
+    if visc_scale != 1.0 or lam_scale != 1.0 or diff_scale != 1.0:
+        import copy
+        tables = copy.copy(tables)
+        tables.visc = tables.visc * visc_scale
+        tables.lam = tables.lam * lam_scale
+        tables.diffbin = tables.diffbin * diff_scale
+    c = CS.Case(cfg, tables)
+    _, u, T, Y = premix_profile()
+    c.init_premix(u, T, Y)
     return c
 
 

@@ -60,6 +60,7 @@ class StxParams(C.Structure):
         ("nrk", C.c_int32),
         ("rhork", C.c_double * 4), ("gamrk", C.c_double * 4),
         ("winf", dp),
+        ("T_wall", C.c_double),
     ]
 
 
@@ -99,6 +100,8 @@ STX_SIGNATURES = [
     ("stx_bcextr_var", _I, [_VP, _VP, _VP]),
     ("stx_bcswap", _I, [_VP, _VP, _VP, _I]),
     ("stx_update_ghost", _I, [_VP, _VP, _VP, _I]),
+    ("stx_update_ghost_aux", _I, [_VP, _VP, _VP, _VP, _I]),
+    ("stx_bc_nr", _I, [_VP, _VP, _VP, _VP, _VP]),
     ("stx_euler_x", _I, [_VP, _VP, _VP, _VP, _I, _I, _I]),
     ("stx_euler_y", _I, [_VP, _VP, _VP, _VP, _I, _I, _I]),
     ("stx_euler_z", _I, [_VP, _VP, _VP, _VP, _I, _I, _I]),
@@ -111,6 +114,7 @@ STX_SIGNATURES = [
     ("stx_update_field", _I, [_VP, _VP, _VP, _VP, _VP]),
     ("stx_rk_finish", _I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _D, _I]),
     ("stx_compute_dt", _I, [_VP, _VP, _VP, _VP, C.POINTER(C.c_double)]),
+    ("stx_compute_residual", _I, [_VP, _VP, _VP, _VP, _VP, _D, C.POINTER(C.c_double)]),
     ("stx_rosenbrock", _I, [_VP, _VP, _VP, _VP, _D, _D, _D]),
     ("stx_rosenbrock_krylov", _I, [_VP, _VP, _VP, _VP, _VP, _D, _D, _D, _I]),
     ("stx_compute_chemistry", _I, [_VP, _VP, _VP, _VP, _VP]),
@@ -141,12 +145,15 @@ ORACLE_SIGNATURES = [
     ("ox_bcextr_var", None, [_VP, _VP]),
     ("ox_bcswap", None, [_VP, _VP, _I]),
     ("ox_update_ghost", None, [_VP, _VP, _I]),
+    ("ox_update_ghost_aux", None, [_VP, _VP, _VP, _I]),
+    ("ox_bc_nr", None, [_VP, _VP, _VP, _VP]),
     ("ox_euler", None, [_VP, _I, _VP, _VP, _VP, _I, _I]),
     ("ox_visflx", None, [_VP, _VP, _VP, _VP, _I]),
     ("ox_init_flux", None, [_VP, _VP, _VP, _D]),
     ("ox_update_flux", None, [_VP, _VP, _VP, _D]),
     ("ox_update_field", None, [_VP, _VP, _VP, _VP]),
     ("ox_compute_dt", None, [_VP, _VP, _VP, C.POINTER(C.c_double)]),
+    ("ox_compute_residual", None, [_VP, _VP, _VP, _VP, _D, C.POINTER(C.c_double)]),
     ("ox_rosenbrock", None, [_VP, _VP, _VP, _D, _D, _D]),
     ("ox_rosenbrock_krylov", None, [_VP, _VP, _VP, _VP, _D, _D, _D, _I]),
     ("ox_compute_chemistry", None, [_VP, _VP, _VP, _VP]),

@@ -189,7 +189,8 @@ class Solver:
 
     # ------------------------------------------------------------------ reference-named calls
     def update_ghost(self, do_swap: int = 1):
-        check(self.lib.stx_update_ghost(self.ctx, self.stream, _p(self.w), do_swap), "update_ghost")
+        check(self.lib.stx_update_ghost_aux(self.ctx, self.stream, _p(self.w), _p(self.w_aux), do_swap),
+              "update_ghost")
 
     def compute_aux(self, central: int = 1, ghost: int = 1):
         check(self.lib.stx_compute_aux(self.ctx, self.stream, _p(self.w), _p(self.w_aux), central, ghost), "compute_aux")

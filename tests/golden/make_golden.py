@@ -74,7 +74,37 @@ def main(ref):
                     pins[name] = float(line.split()[-1].replace("D", "E"))
     pins["ini"] = flame_ini
     dump("flame_log_pins.json", pins)
+    # --- the flame's initial profile (examples/laminar_premix_flame/premix.dat: x, u, T, Y_1..Y_ns per
+    #     cell, read by init_premix, multideal.F90:5534-5606), kept with the package's input data, and the
+    #     run log's progress rows (data.dat:32-131: icyc, step time, dt, time, residual, rho/T/p min/max)
+    pm = np.loadtxt(os.path.join(ex, "laminar_premix_flame", "premix.dat"))
+    out = os.path.join(HERE, "..", "..", "prop-streams2_b200", "stx", "data", "premix_flame_11sp.npz")
+    np.savez_compressed(out, x=pm[:, 0], u=pm[:, 1], T=pm[:, 2], Y=pm[:, 3:].T.copy())
+    print("wrote", os.path.relpath(out, HERE))
+    rows, lines = [], []
+    with open(os.path.join(ex, "laminar_premix_flame", "data.dat")) as fh:
+        for line in fh:
+            f = line.split()
+            if len(f) == 11 and f[0].isdigit():
+                rows.append([int(f[0])] + [float(v) for v in f[1:]])
+                lines.append(line.rstrip("\n"))
+    dump("flame_progress.json", {
+        "source": "examples/laminar_premix_flame/data.dat (reference FP64 GPU run from premix.dat, print_control "
+                  "1000; columns of print_progress, multideal_gpu.F90:1933-1972)",
+        "columns": ["icyc", "step_time", "dt", "time", "residual_rhou", "rhomin", "rhomax", "tmin", "tmax", "pmin",
+                    "pmax"],
+        "rows": rows, "lines": lines})
+    # --- the digitised reference curves of Ferrer et al. that examples/reactive_shock_tube/OUTPUT/result_comp.py
+    #     plots against output_1d_{170,190,230}micro_s.dat (x [m] and T [K], u [m/s], Y_H2)
+    fer = {"source": "examples/reactive_shock_tube/OUTPUT/Ferrer_{Temp,U,YH2}_{170,190,230}micro_s.dat"}
+    for q in ("Temp", "U", "YH2"):
+        for t in (170, 190, 230):
+            a = np.loadtxt(os.path.join(ex, "reactive_shock_tube", "OUTPUT", f"Ferrer_{q}_{t}micro_s.dat"))
+            fer[f"{q}_{t}"] = a.tolist()
+    dump("ferrer_shock_tube.json", fer)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference checkout>")
+    main(sys.argv[1])

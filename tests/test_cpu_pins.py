@@ -191,12 +191,17 @@ def test_ctx_create_rejects_unsupported_options_without_touching_the_gpu():
     case = H.synthetic_case(n=(4, 4, 4))
     par, tab, grid = case.params_struct(), case.tables_struct(), case.grid_struct()
     ctx = C.c_void_p()
-    par.bctags[0] = 6                      # isothermal wall: not on this path
+    par.bctags[0] = 10                     # recycling-rescaling inflow: not on this path
     assert lib.stx_ctx_create(C.byref(par), C.byref(tab), C.byref(grid), C.byref(ctx)) == -4
     par.bctags[0] = 0
-    par.bctags_nr[1] = 1                   # non-reflecting treatment
+    par.bctags_nr[1] = 1                   # characteristic treatment of a periodic face
+    assert lib.stx_ctx_create(C.byref(par), C.byref(tab), C.byref(grid), C.byref(ctx)) == -1
+    par.bctags[0], par.bctags[1] = 2, 2
+    par.bctags_nr[1] = 4                   # not a treatment bc_nr knows
     assert lib.stx_ctx_create(C.byref(par), C.byref(tab), C.byref(grid), C.byref(ctx)) == -4
-    par.bctags_nr[1] = 0
+    par.bctags_nr[1] = 1                   # eul_imax not moved off the face as bc_preproc does
+    assert lib.stx_ctx_create(C.byref(par), C.byref(tab), C.byref(grid), C.byref(ctx)) == -4
+    par.bctags[0], par.bctags[1], par.bctags_nr[1] = 0, 0, 0
     tab.ns = 7                             # species count not compiled in
     assert lib.stx_ctx_create(C.byref(par), C.byref(tab), C.byref(grid), C.byref(ctx)) == -4
     assert lib.stx_ctx_create(None, C.byref(tab), C.byref(grid), C.byref(ctx)) == -1
@@ -205,7 +210,51 @@ def test_ctx_create_rejects_unsupported_options_without_touching_the_gpu():
 
 def test_case_rejects_out_of_scope_inputs():
     cfg = CS.default_ini(4, 4, 4, Y=H.h2air_Y(0.7, H.mechanism("h2air_9sp")))
-    cfg.set("bc", "xmin", 6)
+    cfg.set("bc", "xmin", 10)               # recycling-rescaling inflow
     cfg.set("bc", "xmax", 2)
     with pytest.raises(ValueError):
         CS.Case(cfg, H.tables("h2air_9sp", 101325.0))
+
+
+def _c_struct_fields(hdr, name):
+    """Field names of `typedef struct name { ... } name;` in declaration order."""
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), hdr, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        # "const double *a, *b" / "int32_t bctags[6]" -> a, b / bctags
+        rest = re.sub(r"^(const\s+)?(unsigned\s+)?[A-Za-z_0-9]+\s*", "", decl)
+        for part in rest.split(","):
+            names.append(re.sub(r"[\s*]|\[.*?\]", "", part))
+    return names
+
+
+def _f_type_fields(src, name):
+    body = re.search(r"type, bind\(c\) :: %s\n(.*?)end type %s" % (name, name), src, re.S).group(1)
+    names = []
+    for line in body.splitlines():
+        line = line.split("!", 1)[0].strip()
+        if "::" in line:
+            for part in line.split("::", 1)[1].split(","):
+                names.append(re.sub(r"\(.*?\)|\s", "", part))
+    return [n for n in names if n]
+
+
+def test_fortran_interface_module_matches_the_header():
+    """include/stx_interface.F90 (the iso_c_binding module a Fortran host uses)
+    binds every entry point of include/stx.h, and its derived types list the C
+    structs' fields in the same order (no Fortran compiler here, so this is the
+    check that keeps the two in step)."""
+    hdr = open(os.path.join(H.REPO, "include", "stx.h")).read()
+    src = open(os.path.join(H.REPO, "include", "stx_interface.F90")).read()
+    bound = set(re.findall(r'bind\(c, name="(stx_[a-z0-9_]+)"\)', src))
+    missing = [s for s in _declared_symbols() if s not in bound]
+    assert not missing, missing
+    assert not bound - set(_declared_symbols()), bound - set(_declared_symbols())
+    for st in ("stx_tables", "stx_grid", "stx_params", "stx_fields", "stx_tuning", "stx_kprof"):
+        assert _f_type_fields(src, st) == _c_struct_fields(hdr, st), st
+    for code in re.findall(r"#define (STX_E_[A-Z_]+)\s+(-?\d+)", hdr):
+        assert re.search(r"\b%s = %s\b" % code, src), code

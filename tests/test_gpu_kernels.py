@@ -53,9 +53,14 @@ def S(g):
 
 
 # ------------------------------------------------------------------ aux / ghosts
-@pytest.mark.parametrize("n,bc", [((16, 12, 10), (0, 0, 0, 0, 0, 0)), ((20, 6, 5), (8, 2, 0, 0, 2, 8))])
-def test_update_ghost_and_compute_aux(n, bc):
-    case = H.synthetic_case(n=n, bc=bc, seed=1)
+@pytest.mark.parametrize("n,bc,order,st", [((16, 12, 10), (0, 0, 0, 0, 0, 0), 6, 1), ((20, 6, 5), (8, 2, 0, 0, 2, 8), 6, 1),
+                                         ((16, 12, 10), (0, 0, 0, 0, 0, 0), 2, 0),
+                                         ((16, 12, 10), (0, 0, 0, 0, 0, 0), 4, 1),
+                                         ((16, 12, 10), (8, 2, 0, 0, 2, 8), 8, 0)])
+def test_update_ghost_and_compute_aux(n, bc, order, st):
+    """Ghost fills and eval_aux / eval_aux2; the derivatives of eval_aux2 at every
+    visc_order (= ep_order) the ABI accepts, with both Ducros sensor types."""
+    case = H.synthetic_case(n=n, bc=bc, seed=1, ep_order=order, ng=max(3, order // 2), sensor_type=st)
     g, o = pair(case)
     o.update_ghost(1)
     g.update_ghost(1)
@@ -102,6 +107,18 @@ EULER_CASES = [
     dict(sensor_threshold=-1.0, weno_version=0),         # WENO5-JS characteristic
     dict(sensor_threshold=-1.0, flux_splitting=1),       # WENO5 Rusanov
     dict(sensor_threshold=0.02, sensor_type=0),          # hybrid: both branches present
+    # every other scheme option the ABI accepts (stx_ctx_create: weno_scheme 1..4,
+    # ep_order 2..8 even, nkeep -1..2; ng >= max(ep_order/2, weno_scheme))
+    dict(sensor_threshold=1e9, nkeep=1),                 # central, KEEP(1)
+    dict(sensor_threshold=1e9, nkeep=2, ep_order=2),     # 2nd-order central
+    dict(sensor_threshold=1e9, nkeep=2, ep_order=4),     # 4th-order central
+    dict(sensor_threshold=1e9, nkeep=2, ep_order=8, ng=4),   # 8th-order central (per-face sweep)
+    dict(sensor_threshold=-1.0, weno_scheme=1),          # WENO1 (first-order upwind)
+    dict(sensor_threshold=-1.0, weno_scheme=2),          # WENO3
+    dict(sensor_threshold=-1.0, weno_scheme=4, ng=4),    # WENO7 (per-face sweep)
+    dict(sensor_threshold=-1.0, weno_scheme=2, flux_splitting=1),    # WENO3 Rusanov
+    dict(sensor_threshold=-1.0, weno_scheme=4, flux_splitting=1, ng=4),  # WENO7 Rusanov
+    dict(sensor_threshold=0.02, sensor_type=1, weno_scheme=4, ep_order=8, ng=4),  # hybrid WENO7 / 8th order
 ]
 
 
@@ -136,9 +153,12 @@ def test_euler_overwrite_equals_zero_then_accumulate():
 
 
 # ------------------------------------------------------------------ viscous fluxes
-@pytest.mark.parametrize("n", [(150, 10, 9), (9, 12, 14)])
-def test_visflx(n):
-    case = H.synthetic_case(n=n, seed=6)
+@pytest.mark.parametrize("n,order", [((150, 10, 9), 6), ((9, 12, 14), 6), ((40, 10, 9), 2), ((40, 10, 9), 4),
+                                     ((40, 10, 9), 8)])
+def test_visflx(n, order):
+    """Both viscous modes at every visc_order the ABI accepts (visc_order =
+    ep_order, multideal.F90:683-686; ng = 4 for the 8th-order stencil)."""
+    case = H.synthetic_case(n=n, seed=6, ep_order=order, ng=max(3, order // 2))
     g, o = prime(case)
     rng = np.random.default_rng(7)
     fl0 = rng.standard_normal(o.fl.shape)
@@ -361,3 +381,74 @@ def test_batch_reactor_on_gpu_matches_reference_output():
     assert np.ptp(out, axis=1).max() == 0.0          # identical cells, identical results
     dT = np.abs(out[:, 0] - ref[:300, 2])
     assert dT.max() < 0.02, dT.max()
+
+
+# ------------------------------------------------------------------ remaining ghost tags, bc_nr
+@pytest.mark.parametrize("bc", [(4, 4, 4, 4, 4, 4), (7, 7, 7, 7, 7, 7), (2, 2, 5, 5, 0, 0), (2, 8, 6, 6, 0, 0)])
+def test_update_ghost_remaining_tags(bc):
+    """bcextr_sub (4), bcsym (5, y sides), bcwall (6, isothermal, y sides) and
+    bcoutopenfoam (7) against the oracle, on a field whose velocity has both
+    signs at every face (the outflow fill's switch)."""
+    case = H.synthetic_case(n=(14, 10, 8), bc=bc, seed=11, T_wall=950.0)
+    g, o = pair(case)
+    o.compute_aux(1, 1)            # w_aux (the Newton guesses and mass fractions the fills read)
+    to_gpu(g, o)
+    o.update_ghost(0)
+    g.update_ghost(0)
+    wg, wag = g.host_w(), g.host_w_aux()
+    if 4 in bc or 6 in bc:
+        for m in range(case.nv):
+            H.assert_close(wg[m], o.w[m], 1e-12, f"ghost w[{m}] tags {bc}")
+        for m in range(case.ns):
+            H.assert_close(wag[m], o.w_aux[m], 1e-14, f"w_aux[{m}] tags {bc}")
+    else:
+        assert np.array_equal(wg, o.w)        # copies and sign flips: bit-exact
+    assert not np.array_equal(wg, case.w)    # the fills wrote something
+
+
+NR_CASES = [
+    # (bc tags, bc_nr tags): every treatment on every side
+    ((2, 2, 0, 0, 0, 0), (1, 1, 0, 0, 0, 0)),
+    ((2, 2, 2, 2, 0, 0), (2, 3, 1, 6, 0, 0)),
+    ((0, 0, 2, 2, 2, 2), (0, 0, 3, 2, 6, 1)),
+    ((7, 4, 0, 0, 2, 2), (6, 2, 0, 0, 3, 1)),
+]
+
+
+@pytest.mark.parametrize("bc,nr", NR_CASES)
+def test_bc_nr_matches_oracle(bc, nr):
+    """bc_nr_lat_{x,y,z}: the characteristic treatment added to fl at the
+    boundary cells of each face, against the oracle's dense eigenvector products."""
+    case = H.synthetic_case(n=(14, 10, 8), bc=bc, bc_nr=nr, seed=12)
+    g, o = pair(case)
+    o.update_ghost(1)
+    o.compute_aux(1, 1)
+    to_gpu(g, o)
+    rng = np.random.default_rng(13)
+    fl0 = rng.standard_normal(o.fl.shape)
+    o.fl[:] = fl0
+    g.fl.copy_(torch.from_numpy(fl0))
+    o.lib.ox_bc_nr(o.ctx, vp(o.w_aux), vp(o.w), vp(o.fl))
+    assert g.lib.stx_bc_nr(g.ctx, S(g), vp(g.w_aux), vp(g.w), vp(g.fl)) == 0
+    dg, do = g.fl.cpu().numpy() - fl0, o.fl - fl0
+    assert np.abs(do).max() > 0
+    for m in range(case.nv):
+        H.assert_close(dg[m], do[m], 1e-10, f"bc_nr var {m}", floor=1e-10 * np.abs(do).max())
+
+
+@pytest.mark.parametrize("bc,nr", NR_CASES[1:3])
+def test_steps_with_characteristic_boundaries(bc, nr):
+    """Whole steps (Strang + ROK4, hybrid fluxes, viscous fluxes) with the
+    characteristic boundaries and the convective sweeps cut to eul_*."""
+    case = H.synthetic_case(n=(16, 10, 8), bc=bc, bc_nr=nr, seed=14, cfl=-5e-9)
+    assert case.eul != [1, case.nx, 1, case.ny, 1, case.nz]
+    g, o = pair(case)
+    o.prepare()
+    g.prepare()
+    for _ in range(2):
+        o.step()
+        g.step()
+    wg, wo = case.interior(g.host_w()), case.interior(o.w)
+    for m in range(case.nv):
+        H.assert_close(wg[m], wo[m], 1e-8, f"nr steps w[{m}]",
+                       floor=1e-8 * np.abs(wo[:case.ns]).max() if m < case.ns else None)

@@ -1,0 +1,128 @@
+"""Outputs of the reference's run on the GPU path: the residual / extrema
+reduction of print_progress against the oracle, the restart files (a run
+continued from its restart follows the uninterrupted run), and the
+reactive shock tube run to 230 us with its output_1d_*micro_s.dat files compared
+with the reference curves of Ferrer et al. that the reference's own
+examples/reactive_shock_tube/OUTPUT/result_comp.py plots them against."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from driver import OracleSolver  # noqa: E402
+from stx import configs  # noqa: E402
+from stx import output as O  # noqa: E402
+from stx.solver import Solver  # noqa: E402
+
+
+def test_compute_residual_matches_oracle():
+    """compute_residual_cuf + compute_rho_t_p_minmax_cuf: the extrema exactly,
+    the residual to rounding (the sum is regrouped)."""
+    case = H.synthetic_case(n=(20, 12, 10), seed=31)
+    g = Solver(case)
+    o = OracleSolver(case, threads=8)
+    g.prepare()
+    o.prepare()
+    g.step()
+    o.step()
+    o.w_aux[:] = g.host_w_aux()              # the same fields on both sides
+    o.fln[:] = g.fln.cpu().numpy()
+    out_g = O.compute_residual(g)
+    out_o = (C.c_double * 7)()
+    o.lib.ox_compute_residual(o.ctx, o.fln.ctypes.data_as(C.c_void_p), o.w_aux.ctypes.data_as(C.c_void_p), None,
+                              g.dt, out_o)
+    out_o = list(out_o)
+    assert abs(out_g[0] - out_o[0]) <= 1e-12 * abs(out_o[0])
+    assert out_g[1:] == out_o[1:]
+    # the same call twice gives the same bits (fixed summation order)
+    assert O.compute_residual(g) == out_g
+    g.close()
+
+
+def test_restart_continues_the_run(tmp_path):
+    """A run of 6 steps against 3 steps, a restart written (rst1_*.bin +
+    field_info1.dat, renamed to rst0 / field_info0 as a user does), a new solver
+    that reads it, and 3 more steps.  The restart carries w and the loop state,
+    as the reference's does, but not the Newton iteration's temperature guess
+    (w_aux(J_T) starts again from t0, multideal.F90:3706), so T(e) converges from
+    another start and the two runs agree to the iteration's tolerance amplified
+    by the stiff chemistry, not bit for bit."""
+    case = H.synthetic_case(n=(16, 12, 10), seed=32, T0=1250.0, amp_T=150.0)
+    a = Solver(case)
+    O.run(a, 6, progress=None)
+    b = Solver(case)
+    d = str(tmp_path)
+    O.run(b, 3, outdir=d, print_control=3, progress=None)
+    os.rename(os.path.join(d, O.restart_serial_name()), os.path.join(d, O.restart_serial_name(prefix="rst0")))
+    os.rename(os.path.join(d, "field_info1.dat"), os.path.join(d, "field_info0.dat"))
+    c = Solver(case)
+    st = O.read_restart(c, d)
+    assert c.icyc == 3 and c.time == b.time
+    O.run(c, 3, state=st, progress=None)
+    assert c.icyc == 6 and c.time == a.time
+    wc, wa_ = case.interior(c.host_w()), case.interior(a.host_w())
+    for m in range(case.nv):
+        H.assert_close(wc[m], wa_[m], 1e-8, f"restart w[{m}]",
+                       floor=1e-8 * np.abs(wa_[:case.ns]).max() if m < case.ns else None)
+    # progress.out holds the reference's print_progress line
+    line = open(os.path.join(d, "progress.out")).read().splitlines()[0]
+    assert len(line) == 10 + 18 + 9 * 20 and int(line[:10]) == 3
+    for s in (a, b, c):
+        s.close()
+
+
+FERRER = None
+
+
+def ferrer():
+    global FERRER
+    if FERRER is None:
+        FERRER = H.golden("ferrer_shock_tube.json")
+    return FERRER
+
+
+def compare_with_ferrer(outdir):
+    """For each output time and quantity (T, u, and the output's fourth column,
+    which result_comp.py plots against Ferrer's Y curve): the mean absolute
+    difference at Ferrer's points, over the curve's range."""
+    out = {}
+    for t in (170, 190, 230):
+        a = np.loadtxt(os.path.join(outdir, f"output_1d_{t}micro_s.dat"))
+        for q, col in (("Temp", 1), ("U", 2), ("YH2", 3)):
+            f = np.array(ferrer()[f"{q}_{t}"])
+            ours = np.interp(f[:, 0], a[:, 0], a[:, col])
+            out[f"{q}_{t}"] = float(np.mean(np.abs(ours - f[:, 1])) / (f[:, 1].max() - f[:, 1].min()))
+    return out
+
+
+def test_reference_shock_tube_example_against_ferrer(tmp_path):
+    """examples/reactive_shock_tube as the reference runs it (400 cells, fixed
+    dt = 2e-8 s) to 230 us; the three output files against Ferrer et al."""
+    case = H.shock_tube_case(nx=400)
+    s = Solver(case)
+    O.run(s, 12000, outdir=str(tmp_path), print_control=1000, progress=None, t_end=230e-6)
+    s.close()
+    err = compare_with_ferrer(str(tmp_path))
+    print("FERRER_400", err)
+    assert max(err.values()) < 0.10, err
+
+
+def test_config1_shock_tube_2400_cells_cfl_against_ferrer(tmp_path):
+    """The 1-D reactive shock tube on 2400 cells with CFL 0.5 to t = 230 us."""
+    case = configs.config1_case(2400, cfl=0.5)
+    s = Solver(case)
+    rows = O.run(s, 40000, outdir=str(tmp_path), print_control=1000, progress=None, t_end=230e-6)
+    s.close()
+    assert s.time >= 230e-6 and all(np.isfinite(r).all() for r in map(np.array, rows))
+    err = compare_with_ferrer(str(tmp_path))
+    print("FERRER_2400", err, "steps", s.icyc)
+    assert max(err.values()) < 0.10, err
