@@ -56,6 +56,10 @@ def parse():
                          "flame: the 2000-cell 1-D premixed flame of the reference's published timing; "
                          "serve: a Poisson stream of mixed 0-D / 1-D / 2-D solves")
     ap.add_argument("--graph-steps", type=int, default=10, help="steps per captured graph (--workload flame)")
+    ap.add_argument("--form", default="batched", choices=["batched", "plain"],
+                    help="batched: persistent work-stealing chemistry, staged sweeps with listed WENO faces, "
+                         "autotuned; plain: the reference method's launch structure (a thread per cell for the "
+                         "chemistry, a thread per face for the sweeps, no tuning) -- the same arithmetic")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="fp64: the reference method; mixed: FP32 face fluxes and transport, FP64 residual/chemistry")
     ap.add_argument("--requests", type=int, default=600, help="requests of the served mix (--workload serve)")
@@ -314,7 +318,10 @@ def run_stx(args):
     # launch shapes chosen by the autotuner on the warmed-up fields (the Ducros
     # sensor marks faces by now), timed on this GPU; not part of the timed region
     tuning = None
-    if not args.no_autotune:
+    if args.form == "plain":
+        sol.set_tuning({"sweep_kind": [1, 1, 1], "weno_list": [0, 0, 0], "chem_ctas_per_sm": -1})
+        tuning = dict(sol.tuning(), form="plain")
+    elif not args.no_autotune:
         compute_dt_global()
         tuning = sol.autotune(dt_chem=0.5 * sol.dt)
         torch.cuda.synchronize()
@@ -400,9 +407,13 @@ def run_stx(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
             "data": "synthetic (seeded)",
             "config": config_dict(n, world, {"dt_last": sol.dt, "tuning": tuning,
-                                             "precision_form": "plain FP64" if args.precision == "fp64" else
-                                             "mixed: FP32 central/viscous face fluxes and transport properties, "
-                                             "FP64 RK residual, Newton T(e), WENO faces and chemistry"}),
+                                             "precision_form": "FP64 (the reference method)" if args.precision == "fp64"
+                                             else "mixed: FP32 central/viscous face fluxes and transport properties, "
+                                             "FP64 RK residual, Newton T(e), WENO faces and chemistry",
+                                             "launch_form": "plain: a thread per cell (chemistry) and per face "
+                                             "(sweeps), no tuning" if args.form == "plain" else
+                                             "batched: persistent work-stealing chemistry, staged sweeps with "
+                                             "listed WENO faces, autotuned"}),
             "roofline": roofline, "clocks": ck, "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": wbytes, "d2h_bytes_per_step": wbytes,
                     "path": "stx_advance_solution et al. through the C ABI, state w copied from pinned host memory "
@@ -833,6 +844,7 @@ def run_serve(args):
             "data": "synthetic (seeded)", "config": cfg, "p50_s": stats["p50_s"], "p99_s": stats["p99_s"],
             "by_kind": {k: stats[k] for k in ("reactor", "flame1d", "tube2d") if k in stats},
             "max_grid_in_flight": stats["max_grid_in_flight"], "clocks": ck,
+            "host_calls": stats.get("host_calls"),
             "e2e": {"value": stats["solves_per_s"] * world, "unit": S_METRIC, "path": "host Request objects in, "
                     "host results out (every request's inputs are copied to and its results from the device)"}}
     if rank == 0:

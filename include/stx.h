@@ -305,7 +305,9 @@ typedef struct stx_tuning {
   int32_t sweep_kind[3];     /* convective sweep x, y, z: 0 staged shared-memory tiles, 1 one face per thread */
   int32_t weno_list[3];      /* 1: the faces the Ducros sensor marks are listed and computed by full warps;
                                 0: computed in line by the sweep */
-  int32_t chem_ctas_per_sm;  /* persistent CTAs per SM of the cell chemistry (ROK4); 0: its occupancy limit */
+  int32_t chem_ctas_per_sm;  /* persistent CTAs per SM of the cell chemistry (ROK4); 0: its occupancy limit;
+                                -1: the plain launch, one thread per cell and no work stealing (the
+                                same per-cell arithmetic: the results are the same bit for bit) */
   int32_t chem_ctas_max;     /* out: that occupancy limit */
   int32_t batch_ctas_max;    /* most CTAs of one stx_batch0d_integrate launch; 0: no cap (a server running
                                 several reactor launches at once caps each, leaving room for other work) */

@@ -929,7 +929,7 @@ int stx_set_tuning(stx_ctx *c, const stx_tuning *t) {
   for (int q = 0; q < 3; q++)
     if ((t->sweep_kind[q] != 0 && t->sweep_kind[q] != 1) || (t->weno_list[q] != 0 && t->weno_list[q] != 1))
       return STX_E_INVALID;
-  if (t->chem_ctas_per_sm < 0 || t->batch_ctas_max < 0) return STX_E_INVALID;
+  if (t->chem_ctas_per_sm < -1 || t->batch_ctas_max < 0) return STX_E_INVALID;
   for (int q = 0; q < 3; q++) {
     c->d.p.sweep_kind[q] = t->sweep_kind[q];
     c->weno_list[q] = t->weno_list[q];

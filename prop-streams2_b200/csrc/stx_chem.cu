@@ -34,8 +34,11 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
     t0 = *c.p.time_d;
     t1 = t0 + dttry;
   }
-  for (;;) {
-    long long cell = claim(counter);
+  // counter == nullptr: the plain launch, one thread per cell (cell = global
+  // thread index) and no work stealing; otherwise the persistent grid claims cells
+  const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (bool first = true;; first = false) {
+    long long cell = counter ? claim(counter) : (first ? gt : g.npi);
     if (cell >= g.npi) break;
     int i = 1 + (int)(cell % g.nx);
     long long r = cell / g.nx;
@@ -348,9 +351,14 @@ int chem_ctas_limit(int ns) {
 template <int NS>
 static int rok4_t(const DevCtx &c, const DevCtx *cg, cudaStream_t s, double *w, const double *wa, const double *fl_sav,
                   double dttry, double t0, double t1, int simpler, unsigned int *counter) {
+  long long need = (c.g.npi + chem_block(NS) - 1) / chem_block(NS);
+  if (c.p.chem_ctas_per_sm < 0) {            // the plain launch: a thread per cell, no work stealing
+    k_rok4<NS><<<(unsigned)need, chem_block(NS), 0, s>>>(c, cg, w, wa, fl_sav, dttry, t0, t1, simpler, nullptr);
+    STX_CUDA_TRY(cudaGetLastError());
+    return STX_OK;
+  }
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
   int nb = persistent_blocks((const void *)k_rok4<NS>, chem_block(NS), c.p.chem_ctas_per_sm);
-  long long need = (c.g.npi + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
   k_rok4<NS><<<nb, chem_block(NS), 0, s>>>(c, cg, w, wa, fl_sav, dttry, t0, t1, simpler, counter);
   STX_CUDA_TRY(cudaGetLastError());

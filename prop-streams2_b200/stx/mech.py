@@ -378,13 +378,16 @@ def species_conductivity(sp: Species, T, mu):
 
 
 def binary_diffusion(sa: Species, sb: Species, T, p):
+    """Chapman-Enskog binary diffusion coefficient [m^2/s] at T and p:
+    D_ab = 3/16 sqrt(2 pi (k T)^3 / m_ab) / (p pi sigma_ab^2 Omega11*), with
+    m_ab the reduced mass of one molecule pair."""
     eps = math.sqrt(sa.well_depth * sb.well_depth)
     sig = 0.5 * (sa.diameter + sb.diameter) * 1e-10
     dstar = math.sqrt(_delta_star(sa) * _delta_star(sb))
     ts = T / eps
     om = _omega11(ts) + 0.19 * dstar ** 2 / ts
     mab = (sa.mw * sb.mw / (sa.mw + sb.mw)) / N_AVO
-    return (3.0 / 16.0) * np.sqrt(2.0 * math.pi * K_BOLTZ ** 3 * T ** 3 / mab) / (p * math.pi * sig * sig * om * K_BOLTZ)
+    return (3.0 / 16.0) * np.sqrt(2.0 * math.pi * K_BOLTZ ** 3 * T ** 3 / mab) / (p * math.pi * sig * sig * om)
 
 
 # --------------------------------------------------------------------------- tables

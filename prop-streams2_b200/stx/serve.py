@@ -31,6 +31,7 @@ Latency is completion minus arrival, measured on the host clock.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import dataclasses
 import os
@@ -219,6 +220,20 @@ class Server:
                               device=str(self.device)),
             "tube2d": Solver(configs.tube_case(16, 4, tables=self.tables["tube2d"]), device=str(self.device)),
         }
+        # host time of every call site of the loop: name -> [calls, total s, max s]
+        self.trace: Dict[str, list] = {}
+
+    @contextlib.contextmanager
+    def _timed(self, name: str):
+        t = time.perf_counter()
+        try:
+            yield
+        finally:
+            d = time.perf_counter() - t
+            e = self.trace.setdefault(name, [0, 0.0, 0.0])
+            e[0] += 1
+            e[1] += d
+            e[2] = max(e[2], d)
 
     # ------------------------------------------------------------------ grid solves
     def _case(self, req: Request):
@@ -248,8 +263,10 @@ class Server:
         return 8 * ((case.nv + case.nv_aux) * npg + 3 * case.nv * npi) + (8 << 20)
 
     def _admit_grid(self, req: Request, now: float) -> _GridJob:
-        case = self._case(req)
-        stream = torch.cuda.Stream(self.device)
+        with self._timed("admit.case"):
+            case = self._case(req)
+        with self._timed("admit.stream"):
+            stream = torch.cuda.Stream(self.device)
         staged = []
         with torch.cuda.stream(stream):
             # the host fields go up through pinned pool buffers; a fresh case's
@@ -260,12 +277,15 @@ class Server:
                 v = buf[:a.size].view(a.shape)
                 v.numpy()[...] = a
                 return torch.empty(a.shape, dtype=torch.float64, device=self.device).copy_(v, non_blocking=True)
-            w = up(case.w)
-            w_aux = torch.zeros(case.w_aux.shape, dtype=torch.float64, device=self.device)
-            jT = case.J("T")
-            w_aux[jT].copy_(up(case.w_aux[jT]))
-            sol = Solver(case, device=str(self.device), w=w, w_aux=w_aux, tables_from=self._bases[req.kind])
-            sol.prepare()
+            with self._timed("admit.upload"):
+                w = up(case.w)
+                w_aux = torch.zeros(case.w_aux.shape, dtype=torch.float64, device=self.device)
+                jT = case.J("T")
+                w_aux[jT].copy_(up(case.w_aux[jT]))
+            with self._timed("admit.context"):
+                sol = Solver(case, device=str(self.device), w=w, w_aux=w_aux, tables_from=self._bases[req.kind])
+            with self._timed("admit.prepare"):
+                sol.prepare()
         req.admitted = now
         job = _GridJob(req, sol, stream, self.grid_bytes(case))
         job.staged = staged                  # released when the job ends (the copies are done by then)
@@ -280,18 +300,26 @@ class Server:
             c = job.sol.case
             if self.graphs and n == self.chunk and c.cfl < 0 and c.iter_dt_recompute == 1:
                 if job.graph is None:
-                    job.graph = job.sol.capture(self.chunk)
-                job.sol.replay(job.graph)
+                    with self._timed("advance.capture"):
+                        job.graph = job.sol.capture(self.chunk)
+                with self._timed("advance.replay"):
+                    job.sol.replay(job.graph)
             else:
-                for _ in range(n):
-                    job.sol.step()
-            job.event = torch.cuda.Event()
-            job.event.record(job.stream)
+                with self._timed("advance.steps"):
+                    for _ in range(n):
+                        job.sol.step()
+            with self._timed("advance.event"):
+                job.event = torch.cuda.Event()
+                job.event.record(job.stream)
         job.steps_done += n
 
     def _drain_grid(self, job: _GridJob):
         """Enqueue the result's copies into pinned host buffers (and the status
         word) on the job's stream; the loop completes the job when they land."""
+        with self._timed("drain"):
+            self._drain_grid_(job)
+
+    def _drain_grid_(self, job: _GridJob):
         sol = job.sol
         bw, bt, bs = self.pinned.take(sol.w.numel()), self.pinned.take(sol.w_aux[0].numel()), self.pinned.take(1)
         job.staged += [bw, bt, bs]
@@ -308,6 +336,10 @@ class Server:
         job.host = h
 
     def _finish_grid(self, job: _GridJob, now: float):
+        with self._timed("finish"):
+            self._finish_grid_(job, now)
+
+    def _finish_grid_(self, job: _GridJob, now: float):
         h = job.host
         job.req.result = {"w": h["w"].numpy().copy(), "T": job.sol.case.interior(h["T"].numpy()).copy(),
                           "status": int(h["status"].numpy()[0]) & 0xffffffff}
@@ -344,7 +376,8 @@ class Server:
             # reactor lanes
             for lane in self.lanes:
                 if lane.busy:
-                    k = lane.poll(clock())
+                    with self._timed("reactor.poll"):
+                        k = lane.poll(clock())
                     n_done += k
                     progressed |= k > 0
                 if not lane.busy and pending_r:
@@ -352,12 +385,15 @@ class Server:
                     now = clock()
                     for r in take:
                         r.admitted = now
-                    lane.launch(take, self.t_max, self.max_steps)
+                    with self._timed("reactor.launch"):
+                        lane.launch(take, self.t_max, self.max_steps)
                     progressed = True
             # grid lanes
             still = []
             for job in active:
-                if job.event is None or job.event.query():
+                with self._timed("grid.query"):
+                    ready = job.event is None or job.event.query()
+                if ready:
                     if job.host is not None:             # results have landed
                         self._finish_grid(job, clock())
                         mem_used -= job.nbytes
@@ -388,7 +424,9 @@ class Server:
         lat = np.array([r.latency for r in todo])
         stats = {"requests": len(todo), "makespan_s": makespan, "solves_per_s": len(todo) / makespan,
                  "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                 "max_grid_in_flight": max_active}
+                 "max_grid_in_flight": max_active,
+                 "host_calls": {k: {"calls": v[0], "total_s": round(v[1], 4), "max_ms": round(1e3 * v[2], 2)}
+                                for k, v in sorted(self.trace.items())}}
         for kind in ("reactor", "flame1d", "tube2d"):
             lk = np.array([r.latency for r in todo if r.kind == kind])
             if lk.size:

@@ -71,8 +71,11 @@ def test_listed_weno_and_cta_counts_are_bit_identical():
     w_a, wa_a = _steps(make, BASE, 2)
     w_b, wa_b = _steps(make, dict(BASE, weno_list=[0, 0, 0]), 2)
     w_c, wa_c = _steps(make, dict(BASE, chem_ctas_per_sm=1), 2)
+    # the plain launch: one thread per cell, no work stealing
+    w_d, wa_d = _steps(make, dict(BASE, chem_ctas_per_sm=-1), 2)
     assert np.array_equal(w_a, w_b) and np.array_equal(wa_a, wa_b)
     assert np.array_equal(w_a, w_c) and np.array_equal(wa_a, wa_c)
+    assert np.array_equal(w_a, w_d) and np.array_equal(wa_a, wa_d)
 
 
 @pytest.mark.parametrize("thr", [0.1, -0.2])
