@@ -45,8 +45,8 @@ def parse():
     ap.add_argument("--impl", default="stx", choices=["stx", "reference"])
     ap.add_argument("--n", type=int, default=256, help="cells per direction per GPU")
     ap.add_argument("--seed", type=int, default=1234)
-    ap.add_argument("--cpu-n", type=int, default=32, help="box edge of the CPU sample")
-    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the baseline")
+    ap.add_argument("--cpu-n", type=int, default=64, help="box edge of the CPU sample")
+    ap.add_argument("--cpu-budget", type=float, default=60.0, help="most seconds of timed CPU work for the baseline")
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer leg (default: --steps)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
@@ -78,6 +78,25 @@ def parse():
 # kernel-name prefixes of the HBM-class kernel classes (for --ncu-raw)
 KERNELS_OF_CLASS = {"euler": ("k_euler", "k_weno"), "visc": ("k_visc",), "eval_aux": ("k_eval_aux",),
                     "rk": ("k_update_field", "k_init_flux")}
+
+
+def fp64_peaks(stream_ptr):
+    """The device's FP64 FMA and FP64 tensor-core (DMMA, mma.sync m8n8k4 f64)
+    throughput, measured by libstx_peaks.so (TFLOP/s), or None if it is not built."""
+    import ctypes as C
+    so = os.path.join(ROOT, "prop-streams2_b200", "csrc", "libstx_peaks.so")
+    if not os.path.exists(so):
+        return None
+    lib = C.CDLL(so)
+    lib.stx_peak_fp64.restype = C.c_int
+    lib.stx_peak_fp64.argtypes = [C.c_int, C.c_void_p, C.POINTER(C.c_double)]
+    out = {}
+    for name, which in (("fma_tflops", 0), ("dmma_tflops", 1)):
+        v = C.c_double()
+        out[name] = round(v.value, 2) if lib.stx_peak_fp64(which, C.c_void_p(stream_ptr), C.byref(v)) == 0 else None
+    out["how"] = ("persistent grid of 8 x 256-thread CTAs per SM: 8 chains of dependent DFMA per thread / 4 chains "
+                  "of mma.sync.m8n8k4.f64 per warp; best of 3 timed launches")
+    return out
 
 
 def ncu_traffic(path, prefixes, cells_captured, cells_here):
@@ -175,9 +194,11 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ CPU (oracle) leg
-def cpu_run(n, steps_budget_s, seed, warm=1, threads=None):
-    """The CPU restatement (oracle) on an n^3 same-resolution sample of the workload:
-    returns (cell-steps/s, cores, sample text)."""
+def cpu_run(n, steps, seed, warm=1, budget_s=60.0, threads=None):
+    """The CPU restatement (oracle) on an n^3 same-resolution sample of the workload,
+    with the GPU run's step history: `warm` untimed steps, then `steps` timed steps
+    (fewer if they take longer than budget_s): returns (cell-steps/s, cores, sample
+    text)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     from stx import configs
@@ -193,15 +214,17 @@ def cpu_run(n, steps_budget_s, seed, warm=1, threads=None):
         o.step()
     t0 = time.perf_counter()
     k = 0
-    while True:
+    while k < steps:
         o.step()
         k += 1
         el = time.perf_counter() - t0
-        if el >= steps_budget_s or k >= 1000:
+        if el >= budget_s:
             break
+    el = time.perf_counter() - t0
     o.close()
     rate = n ** 3 * k / el
-    return rate, threads, f"{n}^3 cells (same grid spacing and state statistics), {k} steps after {warm} warm-up, {el:.1f} s"
+    return rate, threads, (f"{n}^3 cells of the same workload (same grid spacing, seed and state statistics), "
+                           f"{k} timed steps after {warm} warm-up steps (the GPU run's step history), {el:.1f} s")
 
 
 def run_reference(args):
@@ -212,8 +235,7 @@ def run_reference(args):
     if not os.path.exists(oracle_so):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
     # W warm-up steps, then K timed steps of the CPU implementation on a bounded sample
-    budget = max(5.0, min(60.0, 6.0 * args.steps))
-    rate, cores, sample = cpu_run(args.cpu_n, budget, args.seed, warm=max(1, min(args.warmup, 2)))
+    rate, cores, sample = cpu_run(args.cpu_n, args.steps, args.seed, warm=args.warmup, budget_s=90.0)
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
@@ -402,6 +424,7 @@ def run_stx(args):
                 "traffic_source": ("ncu capture " + os.path.basename(args.ncu_raw)) if traffic else
                 "null: no ncu capture given (--ncu-raw)"}
 
+    peaks64 = fp64_peaks(torch.cuda.current_stream().cuda_stream) if rank == 0 else None
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
@@ -418,11 +441,14 @@ def run_stx(args):
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": wbytes, "d2h_bytes_per_step": wbytes,
                     "path": "stx_advance_solution et al. through the C ABI, state w copied from pinned host memory "
                             "before and back after every step"},
-            "kernels": cls, "status_bits": status}
+            "kernels": cls, "status_bits": status,
+            "fp64_peaks": peaks64,
+            "chem_bound": "FP64 arithmetic and the per-thread working set, not HBM: see fp64_peaks and the ncu "
+                          "summary of k_rok4 (FP64-pipe utilisation) in profiles/"}
     if args.precision == "mixed" and rank == 0:
         line["error_vs_fp64"] = mixed_error(dev, args.seed)
     if world == 1 and rank == 0 and not args.no_cpu:
-        rate, cores, sample = cpu_run(args.cpu_n, args.cpu_budget, args.seed)
+        rate, cores, sample = cpu_run(args.cpu_n, args.steps, args.seed, warm=args.warmup, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -477,7 +503,9 @@ def cpu_reactors(args, n_sample):
                       vp(T), vp(ti), vp(te), vp(ns))
     el = time.perf_counter() - t0
     lib.ox_ctx_destroy(ctx)
-    return n_sample / el, cores, f"{n_sample} reactors of the same distribution (seed {args.seed}), {el:.1f} s"
+    solved = int((ns <= args.max_steps).sum())
+    return solved / el, cores, (f"{n_sample} reactors of the same distribution (seed {args.seed}), {el:.1f} s; "
+                                f"{solved} solved, {n_sample - solved} at the step cap (counted out, as on the GPU)")
 
 
 def run_reactors(args):
@@ -545,12 +573,22 @@ def run_reactors(args):
     e2e = args.reactors * world * args.steps / (float(ms2.item()) / 1e3)
     h2d = sum(t.numel() * t.element_size() for t in (hT0, hp0, hY0))
     d2h = sum(t.numel() * t.element_size() for t in hout.values())
-    line = {"metric": R_METRIC, "value": value, "unit": R_METRIC, "n_gpus": world, "steps": args.steps,
+    # a reactor is solved when it has run to 2 t_ign or to t_max; the others stop
+    # at the step cap (the slow-induction states: T0 below ~1100 K at several atm,
+    # where ROK4's steps stay small -- the oracle caps the same ones)
+    capped = nsteps > args.max_steps
+    done = int((~capped).sum())
+    line = {"metric": R_METRIC, "value": done * world * args.steps / (ms_max / 1e3), "unit": R_METRIC,
+            "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": reactors_config(args, world),
+            "value_note": "reactors that reached min(2 t_ign, t_max) per second; the launch also carried the capped "
+                          "ones (reactors_launched_per_s)",
+            "reactors_launched_per_s": value,
+            "reactors": {"solved": done, "capped": int(capped.sum()), "per_launch": args.reactors},
             "reactor_steps_per_s": float(nsteps.sum()) * world * args.steps / (ms_max / 1e3),
             "steps_per_reactor": {"mean": float(nsteps.mean()), "max": int(nsteps.max()),
-                                  "capped": int((nsteps > args.max_steps).sum())},
+                                  "capped": int(capped.sum())},
             "ignited": int((t_ign > 0).sum()), "clocks": ck, "gpu_launches": args.steps,
             "e2e": {"value": e2e, "unit": R_METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "BatchReactors.integrate -> stx_batch0d_integrate, inputs from and outputs to pinned "

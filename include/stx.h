@@ -50,6 +50,8 @@ extern "C" {
 #define STX_ST_ROS_STEPS_CAP  0x2u  /* a Rosenbrock cell hit ros_maxsteps */
 #define STX_ST_ROS_TRY_CAP    0x4u  /* a full-Jacobian Rosenbrock step exhausted ros_maxtry */
 #define STX_ST_NONFINITE      0x8u  /* a non-finite value was produced */
+#define STX_ST_WAIT_TIMEOUT   0x10u /* a kernel gave up waiting for its tensor-memory copies (the
+                                       sweep's result is then incomplete); never expected */
 
 /* Property tables: the arrays set_fluid_prop / set_fluid_prop_cantera build
  * (src/multideal/multideal.F90:2714-3318), in their Fortran layouts. */
@@ -132,6 +134,15 @@ int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid 
  * from it.  No counterpart in the reference (one solve per process); for
  * callers that run many solves of one mechanism, e.g. a request server. */
 int stx_ctx_create_like(const stx_ctx *base, const stx_params *par, const stx_grid *grid, stx_ctx **out);
+/* stx_ctx_create_like with the context's uploads (grid, parameters, scratch
+ * zero fills) enqueued on the caller's stream instead of waited for: the call
+ * returns once its pageable host data has been staged, and the context may be
+ * used at once on `stream`, on another stream after `stream` has reached this
+ * point.  Nothing else is synchronised, so a server that admits a request while
+ * other work runs on the device (seconds-long batched reactor launches) does
+ * not wait for that work.  No counterpart in the reference. */
+int stx_ctx_create_like_on(const stx_ctx *base, const stx_params *par, const stx_grid *grid, void *stream,
+                           stx_ctx **out);
 int stx_ctx_destroy(stx_ctx *ctx);
 
 /* Ghost exchange with neighbouring subdomains (the MPI half of the reference's

@@ -17,7 +17,7 @@ module stx_interface
   integer(c_int), parameter :: STX_OK = 0, STX_E_INVALID = -1, STX_E_CUDA = -2, STX_E_NOMEM = -3
   integer(c_int), parameter :: STX_E_UNSUPPORTED = -4, STX_E_TOO_LARGE = -5, STX_E_LOCAL_MEM = -6
   integer(c_int32_t), parameter :: STX_ST_NEWTON_CAP = 1, STX_ST_ROS_STEPS_CAP = 2, STX_ST_ROS_TRY_CAP = 4
-  integer(c_int32_t), parameter :: STX_ST_NONFINITE = 8
+  integer(c_int32_t), parameter :: STX_ST_NONFINITE = 8, STX_ST_WAIT_TIMEOUT = 16
   integer(c_int32_t), parameter :: STX_BC_EXCHANGE = -1
   integer(c_int), parameter :: STX_PREC_FP64 = 0, STX_PREC_MIXED = 1
   integer(c_int), parameter :: STX_NK = 8
@@ -113,6 +113,13 @@ module stx_interface
     integer(c_int) function stx_ctx_create_like(base, par, grid, ctx) bind(c, name="stx_ctx_create_like")
       import :: c_int, c_ptr, stx_params, stx_grid
       type(c_ptr), value           :: base
+      type(stx_params), intent(in) :: par
+      type(stx_grid),   intent(in) :: grid
+      type(c_ptr), intent(out)     :: ctx
+    end function
+    integer(c_int) function stx_ctx_create_like_on(base, par, grid, stream, ctx) bind(c, name="stx_ctx_create_like_on")
+      import :: c_int, c_ptr, stx_params, stx_grid
+      type(c_ptr), value           :: base, stream
       type(stx_params), intent(in) :: par
       type(stx_grid),   intent(in) :: grid
       type(c_ptr), intent(out)     :: ctx

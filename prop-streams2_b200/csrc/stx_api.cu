@@ -28,11 +28,13 @@ struct stx_ctx {
   WenoScratch weno;               // listed WENO faces of the staged sweeps (cap 0: none)
   int weno_list[3];               // per sweep direction: use the listed WENO faces
   std::vector<void *> allocs;
-  // The context's own non-blocking stream: its tables and scratch are allocated,
-  // uploaded and freed stream-ordered on it (cudaMallocFromPoolAsync /
-  // cudaFreeAsync), so creating or destroying a context never waits for other
-  // work on the device (a plain cudaFree synchronises the whole device).
+  // The device's setup stream (setup_stream): the context's tables and scratch
+  // are allocated, uploaded and freed stream-ordered on it
+  // (cudaMallocFromPoolAsync / cudaFreeAsync), so creating or destroying a
+  // context never waits for other work on the device (a plain cudaFree
+  // synchronises the whole device).
   cudaStream_t cs = nullptr;
+  cudaStream_t us = nullptr;      // stream of the creation's uploads: cs, or the caller's (stx_ctx_create_like_on)
   int device;
   // instrumentation (stx_profile_*)
   int prof_on;
@@ -100,16 +102,34 @@ cudaMemPool_t ctx_pool(int dev) {
   return pools[dev];
 }
 
+// The setup stream of a device: one non-blocking stream, created at the first
+// context on the device and kept for the process, that carries only context
+// set-up and tear-down (uploads, zero fills, frees, device-context refreshes).
+// One stream instead of one per context: CUDA maps streams onto a fixed set of
+// hardware queues (CUDA_DEVICE_MAX_CONNECTIONS), and every stream created
+// beyond that shares a queue with an earlier one, whose long-running kernels
+// (a persistent reactor batch runs for seconds) then hold up the set-up work
+// queued behind them -- and the synchronisations that wait for it.
+cudaStream_t setup_stream(int dev) {
+  static std::mutex mu;
+  static std::vector<cudaStream_t> streams;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)streams.size() <= dev) streams.resize(dev + 1, nullptr);
+  if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
+    streams[dev] = nullptr;
+  return streams[dev];
+}
+
 template <typename T>
 int upload(stx_ctx *c, const T *host, size_t n, const T **out) {
   void *p = nullptr;
   if (n == 0) n = 1;
   cudaMemPool_t pool = ctx_pool(c->device);
-  if (!pool || cudaMallocFromPoolAsync(&p, n * sizeof(T), pool, c->cs) != cudaSuccess) return STX_E_NOMEM;
+  if (!pool || cudaMallocFromPoolAsync(&p, n * sizeof(T), pool, c->us) != cudaSuccess) return STX_E_NOMEM;
   c->allocs.push_back(p);
   // pageable host source: the copy is staged before the call returns
-  if (host && cudaMemcpyAsync(p, host, n * sizeof(T), cudaMemcpyHostToDevice, c->cs) != cudaSuccess) return STX_E_CUDA;
-  if (!host && cudaMemsetAsync(p, 0, n * sizeof(T), c->cs) != cudaSuccess) return STX_E_CUDA;
+  if (host && cudaMemcpyAsync(p, host, n * sizeof(T), cudaMemcpyHostToDevice, c->us) != cudaSuccess) return STX_E_CUDA;
+  if (!host && cudaMemsetAsync(p, 0, n * sizeof(T), c->us) != cudaSuccess) return STX_E_CUDA;
   *out = (const T *)p;
   return STX_OK;
 }
@@ -166,13 +186,12 @@ const char *stx_strerror(int code) {
 
 int stx_ctx_destroy(stx_ctx *c) {
   if (!c) return STX_E_INVALID;
-  // stream-ordered frees on the context's stream: the caller has finished its
-  // work on the context's fields (its own streams are synchronised)
-  for (void *p : c->allocs) cudaFreeAsync(p, c->cs);
-  if (c->cs) {
-    cudaStreamSynchronize(c->cs);
-    cudaStreamDestroy(c->cs);
-  }
+  // stream-ordered frees on the setup stream, without waiting for them: the
+  // caller has finished its work on the context (its own streams are
+  // synchronised), and the pool hands the memory out again only to allocations
+  // ordered after the frees
+  if (c->cs)
+    for (void *p : c->allocs) cudaFreeAsync(p, c->cs);
   for (int k = 0; k < STX_NK; k++)
     for (cudaEvent_t e : c->ev[k]) cudaEventDestroy(e);
   delete c;
@@ -182,8 +201,10 @@ int stx_ctx_destroy(stx_ctx *c) {
 }  // extern "C"
 
 // A context from host tables (base null) or on the device tables of base.
+// on: the stream of the uploads (nullptr: the setup stream, and the call
+// returns when they have completed)
 static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const stx_grid *grid, const stx_ctx *base,
-                           stx_ctx **out) {
+                           cudaStream_t on, stx_ctx **out) {
   if (!par || !(tab || base) || !grid || !out) return STX_E_INVALID;
   *out = nullptr;
   const int ns = base ? base->ns : tab->ns, nr = base ? base->d.t.nr : tab->nr;
@@ -222,10 +243,12 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   stx_ctx *c = new (std::nothrow) stx_ctx();
   if (!c) return STX_E_NOMEM;
   cudaGetDevice(&c->device);
-  if (cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking) != cudaSuccess) {
+  c->cs = setup_stream(c->device);
+  if (!c->cs) {
     delete c;
     return STX_E_CUDA;
   }
+  c->us = on ? on : c->cs;
   c->par = *par;
   c->ns = ns;
   c->nv = ns + 4;
@@ -450,7 +473,8 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
     }
   }
   if ((rc = upload<DevCtx>(c, &c->d, 1, &c->dctx_d))) return fail(rc);
-  if (cudaStreamSynchronize(c->cs) != cudaSuccess) return fail(STX_E_CUDA);
+  if (!on && cudaStreamSynchronize(c->cs) != cudaSuccess) return fail(STX_E_CUDA);
+  c->us = c->cs;
   *out = c;
   return STX_OK;
 }
@@ -459,12 +483,18 @@ extern "C" {
 
 int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid *grid, stx_ctx **out) {
   if (!tab) return STX_E_INVALID;
-  return ctx_create_impl(par, tab, grid, nullptr, out);
+  return ctx_create_impl(par, tab, grid, nullptr, nullptr, out);
 }
 
 int stx_ctx_create_like(const stx_ctx *base, const stx_params *par, const stx_grid *grid, stx_ctx **out) {
   if (!base) return STX_E_INVALID;
-  return ctx_create_impl(par, nullptr, grid, base, out);
+  return ctx_create_impl(par, nullptr, grid, base, nullptr, out);
+}
+
+int stx_ctx_create_like_on(const stx_ctx *base, const stx_params *par, const stx_grid *grid, void *stream,
+                           stx_ctx **out) {
+  if (!base || !stream) return STX_E_INVALID;
+  return ctx_create_impl(par, nullptr, grid, base, S(stream), out);
 }
 
 // ------------------------------------------------------------------ aux

@@ -93,7 +93,12 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
 }
 
 // ---------------------------------------------------------------- full Jacobian
-// rosenbrock_rhs (kernels_gpu.F90:9195-9381): updates the cell state in place
+// rosenbrock_rhs (kernels_gpu.F90:9195-9381): updates the cell state in place.
+// The production terms run over the per-reaction sparse stoichiometry lists
+// (chem_source_sp: the same terms in the same order as the dense species
+// loops, so the same bits) with per-thread rows in shared memory: launch with
+// chem_block(NS) threads.  At 53 species / 325 reactions the dense loops read
+// 3 x 53 stoichiometric coefficients per reaction for a handful of non-zeros.
 template <int NS>
 __device__ void ros_rhs(const DevCtx &c, double *wc, double *Y, double &T, double *rhs) {
   const DevTab &t = c.t;
@@ -115,7 +120,17 @@ __device__ void ros_rhs(const DevCtx &c, double *wc, double *Y, double &T, doubl
   T = temp_from_e<NS>(t, c.p, ee, T, Y);
 #pragma unroll
   for (int m = 0; m < NS + 4; m++) rhs[m] = 0.0;
-  chem_source<NS>(t, T, conc, rhs, false);
+  constexpr int CB = chem_block(NS);
+  __shared__ double s_conc[NS * CB], s_rhs[NS * CB];
+  double *cs = s_conc + threadIdx.x, *rs = s_rhs + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    cs[k * CB] = conc[k];
+    rs[k * CB] = 0.0;
+  }
+  chem_source_sp<NS, CB>(t, T, cs, rs);
+#pragma unroll
+  for (int k = 0; k < NS; k++) rhs[k] = rs[k * CB];
 }
 
 template <int NV>
@@ -255,7 +270,7 @@ __device__ void rosenbrock_cell(const DevCtx &c, double *wc, double *Y, double &
 }
 
 template <int NS>
-__global__ void __launch_bounds__(128) k_rosenbrock(DevCtx c, double *__restrict__ w, double *__restrict__ wa,
+__global__ void __launch_bounds__(chem_block(NS)) k_rosenbrock(DevCtx c, double *__restrict__ w, double *__restrict__ wa,
                                                     double dttry, double t0, double t1, unsigned int *counter) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
@@ -369,10 +384,11 @@ template <int NS>
 static int ros_t(const DevCtx &c, cudaStream_t s, double *w, double *wa, double dttry, double t0, double t1,
                  unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
-  int nb = persistent_blocks((const void *)k_rosenbrock<NS>, 128);
-  long long need = (c.g.npi + 127) / 128;
+  constexpr int CB = chem_block(NS);
+  int nb = persistent_blocks((const void *)k_rosenbrock<NS>, CB);
+  long long need = (c.g.npi + CB - 1) / CB;
   if (nb > need) nb = (int)need;
-  k_rosenbrock<NS><<<nb, 128, 0, s>>>(c, w, wa, dttry, t0, t1, counter);
+  k_rosenbrock<NS><<<nb, CB, 0, s>>>(c, w, wa, dttry, t0, t1, counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }

@@ -16,8 +16,15 @@
 //    per stencil point instead of O(ns^2).  The back projection keeps the
 //    reference's summation order.  Results equal the reference's dense
 //    products up to rounding.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <map>
 #include <mutex>
 #include <set>
+#include <tuple>
 #include <utility>
 
 #include "stx_kernels.cuh"
@@ -662,7 +669,7 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const DevC
 #ifndef STX_ETILE_X_MINB
 #define STX_ETILE_X_MINB 5
 #endif
-template <int NS, int DIR> struct ETile {
+template <int NS, int DIR, bool TMA = false> struct ETile {
   static constexpr int TC = DIR == 0 ? 64 : 16;        // cells per line updated by a CTA
   static constexpr int NL = DIR == 0 ? 2 : 16;         // lines per CTA
   static constexpr int H = 3;                          // halo cells each side
@@ -671,17 +678,24 @@ template <int NS, int DIR> struct ETile {
   static constexpr int NP = TC + 3;                    // pair origins per line and distance
   static constexpr int NVC = NS + 7;                   // staged fields
   static constexpr int NT = TC * NL;                   // threads
+  // staged cells of the x sweep's TMA copies: a row of BX cells from an even x
+  // (16-byte rule of tensor copies), landing at a 128-byte-aligned row of RS cells
+  static constexpr int BX = S + 2;
+  static constexpr int RS = TMA ? ((BX * 8 + 127) / 128) * 16 : S;   // row stride of the cell stage
+  static constexpr int VS = DIR == 0 ? NL * RS : S * NL;             // field stride of the cell stage
   // x sweep: the sweep is the contiguous direction, lines are rows (j, k);
   // y / z sweeps: lines are consecutive i
-  __device__ static int sx(int s, int l) { return DIR == 0 ? l * S + s : s * NL + l; }
+  __device__ static int sx(int s, int l) { return DIR == 0 ? l * S + s : s * NL + l; }     // per-cell arrays
+  __device__ static int cx(int s, int l) { return DIR == 0 ? l * RS + s : s * NL + l; }    // the cell stage
   __device__ static int px(int a, int l) { return DIR == 0 ? l * NP + a : a * NL + l; }
   __device__ static int fx(int f, int l) { return DIR == 0 ? l * NF + f : f * NL + l; }
 };
 
-template <int NS, typename R>
+template <int NS, typename R, bool TMA = false>
 __host__ __device__ constexpr size_t etile_smem(int dir) {
-  // cells (double) + faces (R) + pair factors (2 x 3 distances, R) + internal energy (R)
-  return dir == 0 ? (size_t)ETile<NS, 0>::NVC * ETile<NS, 0>::S * ETile<NS, 0>::NL * 8 +
+  // cells (double) + faces (R) + pair factors (2 x 3 distances, R) + internal energy (R);
+  // the TMA stage also takes 128 bytes of alignment slack
+  return dir == 0 ? (size_t)ETile<NS, 0, TMA>::NVC * ETile<NS, 0, TMA>::VS * 8 + (TMA ? 128 : 0) +
                         (size_t)(NS + 4) * ETile<NS, 0>::NF * ETile<NS, 0>::NL * sizeof(R) +
                         (size_t)6 * ETile<NS, 0>::NP * ETile<NS, 0>::NL * sizeof(R) +
                         (size_t)ETile<NS, 0>::S * ETile<NS, 0>::NL * sizeof(R)
@@ -689,6 +703,44 @@ __host__ __device__ constexpr size_t etile_smem(int dir) {
                         (size_t)(NS + 4) * ETile<NS, 1>::NF * ETile<NS, 1>::NL * sizeof(R) +
                         (size_t)6 * ETile<NS, 1>::NP * ETile<NS, 1>::NL * sizeof(R) +
                         (size_t)ETile<NS, 1>::S * ETile<NS, 1>::NL * sizeof(R);
+}
+
+// ---------------------------------------------------------------- tensor-memory-access staging
+// mbarrier and tensor-copy primitives (PTX ISA: mbarrier, cp.async.bulk.tensor).
+// Loads only, into this CTA's own shared memory, from this GPU's own memory, and
+// never with .multicast::cluster.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 2-D tile load of the box at (x, y) of the tensor map into dst, completing on bar
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"((unsigned long long)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+// bounded wait for phase `phase` of bar: false if it did not complete within the limit
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t phase) {
+  for (int it = 0; it < (1 << 22); it++)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
 }
 
 // staged field v -> w_aux field (1-based)
@@ -706,18 +758,26 @@ __device__ __forceinline__ int etile_field(int v) {
   }
 }
 
-template <int NS, int DIR, typename R>
+// TMA (x sweep only): the cell stage is filled by 2-D tensor copies of the
+// staged rows (tmap: w_aux as nxg x (nyg nzg nv_aux) doubles), issued by one
+// thread and completed on an mbarrier; cells outside the ghosted box come back
+// as zeros (the copies' out-of-bounds fill), as the loads of the plain staging
+// give them.  Everything after the staging is the same code on the same values.
+template <int NS, int DIR, typename R, bool TMA = false>
 __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MINB : 2)
     k_euler_tile(DevCtx c, const DevCtx *__restrict__ cg, const double *__restrict__ wa, double *__restrict__ fl,
-                 int nmin, int nmax, int overwrite, const double *__restrict__ fhw, long long cap) {
-  using T = ETile<NS, DIR>;
+                 int nmin, int nmax, int overwrite, const double *__restrict__ fhw, long long cap,
+                 const __grid_constant__ CUtensorMap tmap) {
+  using T = ETile<NS, DIR, TMA>;
   constexpr int TC = T::TC, NL = T::NL, S = T::S, NF = T::NF, NP = T::NP, NVC = T::NVC, NT = T::NT;
   constexpr int NV = NS + 4;
   constexpr int vU = NS, vV = NS + 1, vW = NS + 2, vH = NS + 3, vP = NS + 4, vR = NS + 5, vD = NS + 6;
   const DevGrid &g = c.g;
   extern __shared__ __align__(16) unsigned char e_smem[];
-  double *sc = (double *)e_smem;                          // [NVC][cells]
-  R *sf = (R *)(sc + NVC * S * NL);                       // [NV][faces]
+  unsigned char *sbase = e_smem;
+  if constexpr (TMA) sbase = e_smem + ((128u - (smem_u32(e_smem) & 127u)) & 127u);   // 128-byte aligned rows
+  double *sc = (double *)sbase;                           // [NVC][cells]
+  R *sf = (R *)(sc + NVC * T::VS);                        // [NV][faces]
   R *sup = sf + NV * NF * NL;                             // [3][pairs] mass-flux factor
   R *spe = sup + 3 * NP * NL;                             // [3][pairs] energy term
   R *see = spe + 3 * NP * NL;                             // [cells] internal energy
@@ -733,6 +793,13 @@ __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MIN
   // (x: rows r = blockIdx.x NL + l over (j, k); y / z: i = blockIdx.x NL + l + 1
   // with k resp. j = blockIdx.z + 1)
   __shared__ long long s_gb[NL], s_fb[NL];
+  __shared__ __align__(8) unsigned long long s_bar;
+  if constexpr (TMA) {
+    if (t == 0) {
+      mbar_init(&s_bar, 1);
+      mbar_fence_init();
+    }
+  }
   if (t < NL) {
     const int l = t;
     long long gb = -1, fb = 0;
@@ -760,19 +827,52 @@ __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MIN
     return gb;
   };
   // 1. stage the cells c0-3 .. c0+TC+2 of every line (zero outside the ghosted box)
-  for (int e = t; e < NVC * S * NL; e += NT) {
-    int s, l, v;
-    if (DIR == 0) { s = e % S; l = (e / S) % NL; v = e / (S * NL); }
-    else { l = e % NL; s = (e / NL) % S; v = e / (S * NL); }
-    bool act;
-    long long b = line_base(l, act);
-    int x = c0 - T::H + s;
-    double val = 0.0;
-    if (act && x >= 1 - g.ng && x <= nsw + g.ng) val = FG(wa, b + x * st, etile_field<NS>(v));
-    sc[v * S * NL + T::sx(s, l)] = val;
+  const double *scb = sc;                                 // staged cell 0 of field 0, line 0
+  if constexpr (TMA) {
+    static_assert(DIR == 0, "tensor-copy staging is built for the x sweep");
+    const int xs = c0 - T::H + g.ng - 1;                  // ghosted x index (0-based) of staged cell 0
+    const int x0 = xs & ~1;                               // an even x: 16 bytes of doubles
+    scb = sc + (xs - x0);
+    if (t == 0) {
+      int nact = 0;
+      for (int l = 0; l < NL; l++) nact += s_gb[l] >= 0;
+      fence_proxy_async();                                // the previous reads of this stage come first
+      mbar_expect_tx(&s_bar, (uint32_t)(nact * NVC * T::BX * 8));
+      const long long rows = (long long)g.nyg * g.nzg;
+      for (int l = 0; l < NL; l++) {
+        const long long gb = s_gb[l];
+        if (gb < 0) continue;
+        const long long line = (gb - (g.ng - 1)) / g.nxg;   // (j + ng - 1) + nyg (k + ng - 1)
+        for (int v = 0; v < NVC; v++)
+          tma_load_2d(sc + v * T::VS + l * T::RS, &tmap, &s_bar, x0,
+                      (int)((etile_field<NS>(v) - 1) * rows + line));
+      }
+    }
+    for (int e = t; e < NVC * T::VS; e += NT)             // lines outside the grid: zeros
+      if (s_gb[(e / T::RS) % NL] < 0) sc[e] = 0.0;
+    // every thread waits for the copies (bounded); on a time-out the CTA stops
+    // together and the status word says so
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0));
+    if (!ok) {
+      if (t == 0) set_status(c.p, STX_ST_WAIT_TIMEOUT);
+      mbar_wait_bounded(&s_bar, 0);                       // the copies in flight, once more
+      return;
+    }
+  } else {
+    for (int e = t; e < NVC * S * NL; e += NT) {
+      int s, l, v;
+      if (DIR == 0) { s = e % S; l = (e / S) % NL; v = e / (S * NL); }
+      else { l = e % NL; s = (e / NL) % S; v = e / (S * NL); }
+      bool act;
+      long long b = line_base(l, act);
+      int x = c0 - T::H + s;
+      double val = 0.0;
+      if (act && x >= 1 - g.ng && x <= nsw + g.ng) val = FG(wa, b + x * st, etile_field<NS>(v));
+      sc[v * T::VS + T::cx(s, l)] = val;
+    }
   }
   __syncthreads();
-  auto ld = [&](int v, int s, int l) -> R { return (R)sc[v * S * NL + T::sx(s, l)]; };
+  auto ld = [&](int v, int s, int l) -> R { return (R)scb[v * T::VS + T::cx(s, l)]; };
   const int nkeep = c.p.nkeep;
   int lmax = c.p.ep_order / 2;
   if (lmax < 1) lmax = 1;
@@ -838,7 +938,7 @@ __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MIN
     const int q = fr + 2;
     R *fo = sf + T::fx(fr, l);                            // this face's fluxes, stride NF * NL
     bool shk = false;
-    for (int s = -ws + 1; s <= ws; s++) shk |= (sc[vD * S * NL + T::sx(q + s, l)] > c.p.sensor_threshold);
+    for (int s = -ws + 1; s <= ws; s++) shk |= (scb[vD * T::VS + T::cx(q + s, l)] > c.p.sensor_threshold);
     if (!shk) {
       bool fz = (f == 0 && c.p.fzf[2 * DIR] == 1) || (f == nsw && c.p.fzf[2 * DIR + 1] == 1);
 #pragma unroll 1
@@ -1022,6 +1122,53 @@ long long weno_scratch_faces(const DevGrid &g) {
   return m > d ? m : d;
 }
 
+// The x sweep's tensor map over w_aux (2-D: nxg doubles per row, nyg nzg nv_aux
+// rows; box: one staged row of ETile::BX doubles), encoded through the driver's
+// entry point and cached per (pointer, grid).  No map -- false -- when the
+// layout breaks a rule of tensor copies (a row stride that is not a multiple of
+// 16 bytes, i.e. odd nxg; a base that is not 16-byte aligned; more rows than a
+// 32-bit coordinate) or the entry point is missing: the sweep then stages with
+// plain loads.  STX_TMA=0 turns the tensor copies off.
+static bool xsweep_tmap(const DevGrid &g, int nv_aux, const double *wa, CUtensorMap *out) {
+  static std::mutex mu;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static bool tried = false, off = false;
+  static std::map<std::tuple<uintptr_t, int, int, int, int>, CUtensorMap> cache;
+  const long long rows = (long long)g.nyg * g.nzg * nv_aux;
+  if ((g.nxg & 1) || (((uintptr_t)wa) & 15) || rows >= 0x7fffffffLL) return false;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!tried) {
+    tried = true;
+    const char *env = std::getenv("STX_TMA");
+    off = env && std::strcmp(env, "0") == 0;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (!off && cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  if (off || !encode) return false;
+  auto key = std::make_tuple((uintptr_t)wa, g.nxg, g.nyg, g.nzg, nv_aux);
+  auto it = cache.find(key);
+  if (it != cache.end()) {
+    *out = it->second;
+    return true;
+  }
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)g.nxg, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)g.nxg * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)ETile<9, 0, true>::BX, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  if (encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)wa, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  if (cache.size() > 64) cache.clear();
+  cache[key] = m;
+  *out = m;
+  return true;
+}
+
 template <int NS, int DIR, typename R>
 static int euler_tile_launch(const DevCtx &c, const DevCtx *cg, cudaStream_t s, const double *wa, double *fl,
                              int nmin, int nmax, int ow, const WenoScratch *wsc) {
@@ -1054,7 +1201,17 @@ static int euler_tile_launch(const DevCtx &c, const DevCtx *cg, cudaStream_t s, 
   if (lgrp > 0x7fffffffLL || tiles > 65535 || other > 65535) return STX_E_INVALID;
   // sweep tiles in gridDim.y: the tiles that share halos run close together
   dim3 grid((unsigned)lgrp, (unsigned)tiles, (unsigned)other);
-  k_euler_tile<NS, DIR, R><<<grid, T::NT, smem, s>>>(c, cg, wa, fl, nmin, nmax, ow, fhw, cap);
+  CUtensorMap tm;
+  std::memset(&tm, 0, sizeof(tm));
+  bool tma = false;
+  if constexpr (DIR == 0) {
+    if (xsweep_tmap(g, c.p.nv_aux, wa, &tm)) {
+      tma = true;
+      k_euler_tile<NS, 0, R, true><<<grid, T::NT, etile_smem<NS, R, true>(0), s>>>(c, cg, wa, fl, nmin, nmax, ow,
+                                                                                   fhw, cap, tm);
+    }
+  }
+  if (!tma) k_euler_tile<NS, DIR, R><<<grid, T::NT, smem, s>>>(c, cg, wa, fl, nmin, nmax, ow, fhw, cap, tm);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
@@ -1111,6 +1268,10 @@ static int euler_setup_t() {
                                       (int)etile_smem<NS, double>(2)));
     STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)etile_smem<NS, float>(0)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 0, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, double, true>(0)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 0, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, float, true>(0)));
     STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)etile_smem<NS, float>(1)));
     STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -92,6 +92,7 @@ STX_SIGNATURES = [
     ("stx_strerror", C.c_char_p, [_I]),
     ("stx_ctx_create", _I, [C.POINTER(StxParams), C.POINTER(StxTables), C.POINTER(StxGrid), C.POINTER(_VP)]),
     ("stx_ctx_create_like", _I, [_VP, C.POINTER(StxParams), C.POINTER(StxGrid), C.POINTER(_VP)]),
+    ("stx_ctx_create_like_on", _I, [_VP, C.POINTER(StxParams), C.POINTER(StxGrid), _VP, C.POINTER(_VP)]),
     ("stx_set_exchange", _I, [_VP, EXCHANGE_FN, _VP]),
     ("stx_ctx_destroy", _I, [_VP]),
     ("stx_eval_aux", _I, [_VP, _VP, _VP, _VP, _I, _I, _I, _I, _I, _I]),

@@ -185,17 +185,31 @@ class Server:
     within the reactors the warp-per-reactor kernel runs at once on a B200, so
     every served batch, like a request served alone, takes that kernel)."""
 
-    def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 32, chunk: int = 5,
-                 reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 16,
+    # torch hands out the streams of a per-device pool of 32 in turn; the
+    # lanes' and the grid solves' streams must all be distinct
+    STREAM_POOL = 32
+
+    def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 20, chunk: int = 5,
+                 reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 12,
                  graphs: bool = True):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         torch.cuda.set_device(self.device)
+        if reactor_lanes + max_grid > self.STREAM_POOL:
+            raise ValueError(f"reactor_lanes + max_grid must be at most {self.STREAM_POOL}: torch's stream pool "
+                             "would hand a grid solve the stream of a reactor lane")
         rtab = M.build_tables(configs.mechanism("h2air_9sp"), 101325.0, 200.0, 5500.0, 1.0)
         self.lanes = [_ReactorLane(BatchReactors("h2air_9sp", device=str(self.device), tables=rtab),
                                    torch.cuda.Stream(self.device), reactor_batch) for _ in range(reactor_lanes)]
         self.reactors = self.lanes[0].br
+        # the grid solves' streams, created once: every stream created beyond
+        # CUDA_DEVICE_MAX_CONNECTIONS shares a hardware queue with an earlier one,
+        # and work queued behind a reactor lane's seconds-long launch in a shared
+        # queue waits for it, so the loop creates no stream while it serves
+        self._streams = [torch.cuda.Stream(self.device) for _ in range(max_grid)]
+        conns = int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8"))
+        self.stream_budget = {"reactor_lanes": reactor_lanes, "grid_streams": max_grid, "connections": conns}
         # the lanes' persistent kernels together hold at most one CTA per SM
         # (half the warp kernel's occupancy), so the grid solves' kernels keep
         # finding room on every SM
@@ -265,8 +279,7 @@ class Server:
     def _admit_grid(self, req: Request, now: float) -> _GridJob:
         with self._timed("admit.case"):
             case = self._case(req)
-        with self._timed("admit.stream"):
-            stream = torch.cuda.Stream(self.device)
+        stream = self._streams.pop()
         staged = []
         with torch.cuda.stream(stream):
             # the host fields go up through pinned pool buffers; a fresh case's
@@ -283,7 +296,8 @@ class Server:
                 jT = case.J("T")
                 w_aux[jT].copy_(up(case.w_aux[jT]))
             with self._timed("admit.context"):
-                sol = Solver(case, device=str(self.device), w=w, w_aux=w_aux, tables_from=self._bases[req.kind])
+                sol = Solver(case, device=str(self.device), w=w, w_aux=w_aux, tables_from=self._bases[req.kind],
+                             stream_ordered=True)
             with self._timed("admit.prepare"):
                 sol.prepare()
         req.admitted = now
@@ -348,6 +362,7 @@ class Server:
         for b in job.staged:
             self.pinned.give(b)
         job.staged = []
+        self._streams.append(job.stream)
 
     # ------------------------------------------------------------------ the loop
     def run(self, requests: List[Request], realtime: bool = True, poll_s: float = 2e-4) -> Dict:

@@ -27,13 +27,17 @@ def _p(t: Optional[torch.Tensor]):
 class Solver:
     def __init__(self, case, device: str = "cuda", w: Optional[torch.Tensor] = None,
                  w_aux: Optional[torch.Tensor] = None, aux_slots: Optional[Sequence[int]] = None,
-                 tables_from: Optional["Solver"] = None):
+                 tables_from: Optional["Solver"] = None, stream_ordered: bool = False):
         """case: a Case; w, w_aux: device fields to use in place of the case's host
         fields.  aux_slots: upload only these (0-based) slots of case.w_aux, the
         others starting at zero -- for a fresh case only the temperature slot
         (the Newton iteration's first guess) holds data before eval_aux.
         tables_from: a live solver of the same mechanism whose device tables
-        this one uses (stx_ctx_create_like); it must outlive this one."""
+        this one uses (stx_ctx_create_like); it must outlive this one.
+        stream_ordered (with tables_from): the context's uploads are enqueued on
+        the current stream instead of waited for (stx_ctx_create_like_on), so
+        creating the solver waits for no other work on the device; use it on
+        that stream."""
         if not torch.cuda.is_available():
             raise RuntimeError("the stx solver needs a CUDA device (there is no CPU fallback)")
         self.lib = load_stx()
@@ -48,8 +52,12 @@ class Solver:
         if tables_from is not None:
             if tables_from.case.ns != case.ns or not tables_from.ctx:
                 raise ValueError("tables_from must be a live solver of the same mechanism")
-            check(self.lib.stx_ctx_create_like(tables_from.ctx, C.byref(self._par), C.byref(self._grid), C.byref(ctx)),
-                  "stx_ctx_create_like")
+            if stream_ordered:
+                check(self.lib.stx_ctx_create_like_on(tables_from.ctx, C.byref(self._par), C.byref(self._grid),
+                                                      self.stream, C.byref(ctx)), "stx_ctx_create_like_on")
+            else:
+                check(self.lib.stx_ctx_create_like(tables_from.ctx, C.byref(self._par), C.byref(self._grid),
+                                                   C.byref(ctx)), "stx_ctx_create_like")
         else:
             check(self.lib.stx_ctx_create(C.byref(self._par), C.byref(self._tab), C.byref(self._grid), C.byref(ctx)),
                   "stx_ctx_create")
