@@ -51,11 +51,12 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--stiff-n", type=int, default=16, help="box edge of --workload stiff53")
-    ap.add_argument("--workload", default="turbulence", choices=["turbulence", "reactors", "flame", "serve", "stiff53"],
+    ap.add_argument("--workload", default="turbulence",
+                    choices=["turbulence", "reactors", "flame", "serve", "stiff53", "tube"],
                     help="turbulence: the headline reacting-step benchmark; reactors: batched 0-D reactors; "
                          "flame: the 2000-cell 1-D premixed flame of the reference's published timing; "
                          "serve: a Poisson stream of mixed 0-D / 1-D / 2-D solves")
-    ap.add_argument("--graph-steps", type=int, default=10, help="steps per captured graph (--workload flame)")
+    ap.add_argument("--graph-steps", type=int, default=10, help="steps per captured graph (--workload flame, tube)")
     ap.add_argument("--form", default="batched", choices=["batched", "plain"],
                     help="batched: persistent work-stealing chemistry, staged sweeps with listed WENO faces, "
                          "autotuned; plain: the reference method's launch structure (a thread per cell for the "
@@ -731,6 +732,128 @@ def run_flame(args):
     return 0
 
 
+# ------------------------------------------------------------------ config 1: CFL-driven shock tube
+TUBE_N = 2400
+
+
+def tube_config(world, graph_steps):
+    return {"workload": f"1-D reactive shock tube, {TUBE_N} cells over 0.12 m, 9 species / 18 reactions "
+                        "(examples/reactive_shock_tube's mechanism and initial state, H2:O2:Ar = 2:1:7): reflecting "
+                        "wall at x = 0, extrapolation at 0.12 m, WENO5-Z everywhere, Strang + ROK4, Wray RK3, "
+                        "CFL 0.5 (dt recomputed every step), from t = 0",
+            "cells_per_gpu": TUBE_N, "species": 9, "reactions": 18, "precision_form": "plain FP64",
+            "parallelism": f"dp{world} (independent tubes)",
+            "launch": f"{graph_steps} CFL-driven steps per CUDA graph launch (dt formed on the device)",
+            "l2": "fields fit in L2; latency bound"}
+
+
+def cpu_tube(budget_s=20.0):
+    """The oracle on the same tube, all host cores, for about budget_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    oracle_so = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.exists(oracle_so):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    from stx import configs
+    from driver import OracleSolver
+    cores = os.cpu_count() or 1
+    o = OracleSolver(configs.config1_case(TUBE_N, cfl=0.5), threads=cores)
+    o.prepare()
+    o.step()
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        o.step()
+        k += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or k >= 5000:
+            break
+    o.close()
+    return TUBE_N * k / el, cores, f"the same {TUBE_N}-cell tube, {k} CFL-driven steps after 1 warm-up, {el:.1f} s"
+
+
+def run_tube(args):
+    import torch
+    import torch.distributed as dist
+    from stx import configs
+    from stx.solver import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    G = max(1, args.graph_steps)
+    K = max(G, (args.steps // G) * G)
+    W = max(3, args.warmup)
+
+    def timed(fn, n):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        return float(ms.item())
+
+    # captured: G CFL-driven steps per graph launch (every replay reads the time back)
+    sol = Solver(configs.config1_case(TUBE_N, cfl=0.5), device=str(dev))
+    sol.prepare()
+    for _ in range(W):
+        sol.step()
+    g = sol.capture(G)
+    sol.replay(g)
+    clocks = Clocks(local)
+    clocks.start()
+    ms_graph = timed(lambda: sol.replay(g), K // G)
+    ck = clocks.stop()
+    value = TUBE_N * world * K / (ms_graph / 1e3)
+    t_end, status = sol.time, sol.status()
+    # the host loop: the nine CFL maxima read back every step (Solver.step)
+    ms_host = timed(sol.step, K)
+    host = TUBE_N * world * K / (ms_host / 1e3)
+    # e2e: graph replays with the state from pinned host memory before and back after every replay
+    host_w = torch.empty(sol.w.shape, dtype=torch.float64, pin_memory=True)
+    host_w.copy_(sol.w)
+
+    def e2e_chunk():
+        sol.w.copy_(host_w, non_blocking=True)
+        sol.replay(g)
+        host_w.copy_(sol.w, non_blocking=True)
+    ms_e2e = timed(e2e_chunk, K // G)
+    e2e = TUBE_N * world * K / (ms_e2e / 1e3)
+    wbytes = sol.w.numel() * 8
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_graph / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "the reference example's initial state (synthetic grid of 2400 cells)",
+            "config": tube_config(world, G), "clocks": ck, "gpu_launches": K // G,
+            "host_loop": {"value": host, "ms_per_step": ms_host / K,
+                          "path": "Solver.step: the CFL maxima read back to the host every step"},
+            "sim_time_after_timed_steps_s": t_end,
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": wbytes / G, "d2h_bytes_per_step": wbytes / G,
+                    "path": "graph replays through the C ABI, state w from pinned host memory before and back "
+                            "after every replay of G steps"},
+            "status_bits": status}
+    if world == 1 and rank == 0 and not args.no_cpu:
+        rate, cores, sample = cpu_tube()
+        line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------------ 53-species stiff mechanism
 def stiff_config(n, world):
     return {"workload": f"synthetic stiff-mechanism box, {n}^3 cells per GPU: 53 species / 325 seeded reactions "
@@ -914,6 +1037,21 @@ def main():
                                       "d2h_bytes_per_step": 0}}), flush=True)
             return 0
         return run_flame(args)
+    if args.workload == "tube":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) != 0:
+                return 0
+            rate, cores, sample = cpu_tube()
+            print(json.dumps({"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC,
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "the reference example's initial state", "config": tube_config(args.gpus, 1),
+                              "cpu_baseline": {"value": rate, "unit": METRIC, "cores": cores, "kind": "port",
+                                               "sample": sample},
+                              "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
+        return run_tube(args)
     if args.workload == "stiff53":
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) != 0:

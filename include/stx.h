@@ -260,7 +260,17 @@ int stx_set_precision(stx_ctx *ctx, int mode);
  * holds the field pointers and the context: keep both alive while it exists. */
 typedef struct stx_graph stx_graph;
 int stx_graph_create(stx_ctx *ctx, const stx_fields *f, double dt, int nsteps, stx_graph **out);
+/* Captured steps for CFL-driven runs (cfl > 0, iter_dt_recompute = 1): each
+ * captured step also forms the nine CFL maxima (compute_dt_cuf,
+ * kernels_gpu.F90:6075-6152) and dt = cfl / max in device memory, which the
+ * step's kernels read (the reference reads the maxima back to its host loop,
+ * multideal_gpu.F90:1756), so nsteps steps replay with no host round trip and
+ * give the step-by-step results bit for bit.  One rank only (no exchange). */
+int stx_graph_create_cfl(stx_ctx *ctx, const stx_fields *f, double cfl, int nsteps, stx_graph **out);
 int stx_graph_launch(stx_graph *g, void *stream, double time);
+/* After a launch on `stream`: the simulation time and the last step size (the
+ * fixed dt of a fixed-dt graph).  Synchronises the stream. */
+int stx_graph_state(stx_graph *g, void *stream, double *time, double *dt);
 int stx_graph_destroy(stx_graph *g);
 
 /* n independent adiabatic constant-pressure 0-D reactors integrated by ROK4 in

@@ -318,6 +318,19 @@ module stx_interface
       integer(c_int), value :: nsteps
       type(c_ptr), intent(out) :: g
     end function
+    integer(c_int) function stx_graph_create_cfl(ctx, f, cfl, nsteps, g) bind(c, name="stx_graph_create_cfl")
+      import :: c_int, c_ptr, c_double, stx_fields
+      type(c_ptr), value :: ctx
+      type(stx_fields), intent(in) :: f
+      real(c_double), value :: cfl
+      integer(c_int), value :: nsteps
+      type(c_ptr), intent(out) :: g
+    end function
+    integer(c_int) function stx_graph_state(g, stream, time, dt) bind(c, name="stx_graph_state")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: g, stream
+      real(c_double), intent(out) :: time, dt
+    end function
     integer(c_int) function stx_graph_launch(g, stream, time) bind(c, name="stx_graph_launch")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: g, stream

@@ -22,6 +22,7 @@ struct stx_ctx {
   double *res_d;                  // residual partial sums (STX_RES_BLOCKS) of stx_compute_residual
   unsigned long long *mm_d;       // its six rho / T / p extrema
   double *time_d;                 // simulation time of captured steps (stx_graph_*)
+  double *dtv_d;                  // step size of captured CFL-driven steps (stx_graph_create_cfl)
   const DevCtx *dctx_d;           // device copy of d, for device functions that take the context by reference
   stx_exchange_fn xfn = nullptr;   // ghost exchange at STX_BC_EXCHANGE faces (stx_set_exchange)
   void *xuser = nullptr;
@@ -425,7 +426,7 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   if ((rc = upload<unsigned int>(c, nullptr, 1, &cn))) return fail(rc);
   if ((rc = upload<unsigned long long>(c, nullptr, 9, &dtp))) return fail(rc);
   const double *tm = nullptr;
-  if ((rc = upload<double>(c, nullptr, 1, &tm))) return fail(rc);
+  if ((rc = upload<double>(c, nullptr, 2, &tm))) return fail(rc);   // time, dt of captured steps
   const double *rp = nullptr;
   const unsigned long long *mmp = nullptr;
   if ((rc = upload<double>(c, nullptr, STX_RES_BLOCKS, &rp))) return fail(rc);
@@ -436,6 +437,7 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   c->counter_d = (unsigned int *)cn;
   c->dt_d = (unsigned long long *)dtp;
   c->time_d = (double *)tm;
+  c->dtv_d = (double *)tm + 1;
   p.status = c->status_d;
   {
     const char *ek = std::getenv("STX_EULER_KERNEL");
@@ -770,23 +772,43 @@ static int rhs_pass(stx_ctx *c, void *s, const stx_fields *f) {
   return STX_OK;
 }
 
-int stx_rk_sync(stx_ctx *c, void *s, const stx_fields *f, double dt, int simpler) {
-  if (!c || !f || !f->w || !f->w_aux || !f->fl || !f->fln || (simpler == 1 && !f->fl_sav)) return STX_E_INVALID;
+// rk_sync (multideal_gpu.F90:548-621).  scale: the factor of dt that the
+// splitting hands this call (1, or 0.5 for the simpler splitting's RK half);
+// used only while a CFL-driven step is captured (c->d.p.dt_d set), where the
+// kernels form the RK scalars from the device dt.
+static int rk_sync_impl(stx_ctx *c, void *s, const stx_fields *f, double dt, int simpler, double scale) {
+  const bool dev = c->d.p.dt_d != nullptr;
   for (int istep = 0; istep < c->par.nrk; istep++) {
-    double rhodt = c->par.rhork[istep] * dt;
-    double gamdt = c->par.gamrk[istep] * dt;
-    if (simpler == 1) TRY(stx_init_flux_simpler(c, s, f->fl, f->fln, f->fl_sav, rhodt));
-    else TRY(stx_init_flux(c, s, f->fl, f->fln, rhodt));
+    double rhodt = dev ? c->par.rhork[istep] : c->par.rhork[istep] * dt;
+    double gamdt = dev ? c->par.gamrk[istep] : c->par.gamrk[istep] * dt;
+    {
+      Prof pf(c, S(s), STX_K_RK, 1, simpler == 1 ? 0.0 : (double)c->d.g.npi * B8(3 * c->nv));
+      TRY(launch_init_flux(c->d, S(s), f->fl, f->fln, simpler == 1 ? f->fl_sav : nullptr, rhodt, scale));
+    }
     TRY(rhs_pass(c, s, f));
-    TRY(stx_rk_finish(c, s, f->w, f->fl, f->fln, f->fl_sav, f->fluid_mask, gamdt, simpler));
+    {
+      Prof pf(c, S(s), STX_K_RK, 1, (double)c->d.g.npi * B8((simpler == 1 ? 6 : 5) * c->nv));
+      TRY(launch_update_field(c->d, S(s), f->w, f->fl, f->fln, simpler == 1 ? f->fl_sav : nullptr, f->fluid_mask,
+                              gamdt, 1, scale));
+    }
     TRY(stx_update_ghost_aux(c, s, f->w, f->w_aux, 0));
   }
   return STX_OK;
 }
 
+int stx_rk_sync(stx_ctx *c, void *s, const stx_fields *f, double dt, int simpler) {
+  if (!c || !f || !f->w || !f->w_aux || !f->fl || !f->fln || (simpler == 1 && !f->fl_sav)) return STX_E_INVALID;
+  return rk_sync_impl(c, s, f, dt, simpler, 1.0);
+}
+
+// advance_solution (multideal_gpu.F90:1605-1642).  While a CFL-driven step is
+// captured, dt is not known on the host: the chemistry receives the splitting's
+// factor of dt as its dttry (the kernels scale it by the device dt) and the RK
+// half its scale.
 int stx_advance_solution(stx_ctx *c, void *s, const stx_fields *f, double dt, double time) {
   if (!c || !f || !f->w || !f->w_aux || !f->fl || !f->fln) return STX_E_INVALID;
   const stx_params &p = c->par;
+  const bool dev = c->d.p.dt_d != nullptr;
   if (p.enable_chemistry == 2) {
     if (p.operator_splitting == 1) {
       if (p.rosenbrock_version != 2 || !f->fl_sav) return STX_E_INVALID;
@@ -797,19 +819,20 @@ int stx_advance_solution(stx_ctx *c, void *s, const stx_fields *f, double dt, do
       TRY(stx_update_ghost_aux(c, s, f->w, f->w_aux, 0));
       TRY(stx_sav_flx(c, s, f->fl, f->fl_sav));
       TRY(stx_compute_aux(c, s, f->w, f->w_aux, 1, 0));
-      TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, f->fl_sav, dt_chem, time, time + dt_chem, 1));
-      TRY(stx_rk_sync(c, s, f, 0.5 * dt, 1));
+      TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, f->fl_sav, dev ? 1.0 : dt_chem, time, time + dt_chem, 1));
+      TRY(rk_sync_impl(c, s, f, 0.5 * dt, 1, 0.5));
     } else {
       double dt_chem = 0.5 * dt;
-      if (p.rosenbrock_version == 1) TRY(stx_rosenbrock(c, s, f->w, f->w_aux, dt_chem, time, time + dt_chem));
-      else TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, nullptr, dt_chem, time, time + dt_chem, 0));
-      TRY(stx_rk_sync(c, s, f, dt, 0));
+      const double tr = dev ? 0.5 : dt_chem;
+      if (p.rosenbrock_version == 1) TRY(stx_rosenbrock(c, s, f->w, f->w_aux, tr, time, time + dt_chem));
+      else TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, nullptr, tr, time, time + dt_chem, 0));
+      TRY(rk_sync_impl(c, s, f, dt, 0, 1.0));
       TRY(stx_compute_aux(c, s, f->w, f->w_aux, 1, 0));
-      if (p.rosenbrock_version == 1) TRY(stx_rosenbrock(c, s, f->w, f->w_aux, dt_chem, time, time + dt_chem));
-      else TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, nullptr, dt_chem, time, time + dt_chem, 0));
+      if (p.rosenbrock_version == 1) TRY(stx_rosenbrock(c, s, f->w, f->w_aux, tr, time, time + dt_chem));
+      else TRY(stx_rosenbrock_krylov(c, s, f->w, f->w_aux, nullptr, tr, time, time + dt_chem, 0));
     }
   } else {
-    TRY(stx_rk_sync(c, s, f, dt, 0));
+    TRY(rk_sync_impl(c, s, f, dt, 0, 1.0));
   }
   return STX_OK;
 }
@@ -830,43 +853,61 @@ int stx_set_precision(stx_ctx *c, int mode) {
 // the time advance) are captured once into a CUDA graph whose chemistry
 // kernels read the time from c->time_d and whose last node advances it, so
 // one graph launch replaces ~50 launches per step with the same arithmetic.
+//
+// A CFL-driven run (cfl > 0, dt recomputed every step) is captured the same
+// way with the step size in device memory as well: each step forms the nine
+// CFL maxima (compute_dt_cuf) and dt = cfl / max on the device, and the
+// kernels that take a dt-derived scalar form it from there (DevPar::dt_d), so
+// nothing returns to the host between steps; stx_graph_state reads the time
+// and the last dt back after a launch.
 struct stx_graph {
   stx_ctx *c;
   cudaGraphExec_t exec;
-  double dt;
+  double dt;          // fixed dt, or 0 for a CFL-driven graph
+  double cfl;
   int nsteps;
 };
 
 namespace {
 __global__ void k_time_add(double *t, double dt) { *t = *t + dt; }
 __global__ void k_time_set(double *t, double v) { *t = v; }
-}  // namespace
 
-int stx_graph_create(stx_ctx *c, const stx_fields *f, double dt, int nsteps, stx_graph **out) {
-  if (!c || !f || !out || nsteps < 1 || !(dt > 0.0)) return STX_E_INVALID;
+// dt > 0: fixed step; otherwise cfl > 0 and the step comes from the CFL maxima
+int graph_create_impl(stx_ctx *c, const stx_fields *f, double dt, double cfl, int nsteps, stx_graph **out) {
   *out = nullptr;
   if (c->xfn) return STX_E_UNSUPPORTED;   // the exchange runs host code at every swap
+  const bool dev = !(dt > 0.0);
   cudaStream_t cs;
   STX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   const int prof = c->prof_on;
   c->prof_on = 0;
   c->d.p.time_d = c->time_d;
+  if (dev) c->d.p.dt_d = c->dtv_d;
   int rc = STX_OK;
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) rc = STX_E_CUDA;
   for (int n = 0; n < nsteps && rc == STX_OK; n++) {
     if ((rc = stx_compute_aux(c, cs, f->w, f->w_aux, 1, 0))) break;
+    if (dev) {
+      if ((rc = launch_compute_dt(c->d, cs, f->w_aux, f->fluid_mask, c->dt_d))) break;
+      if ((rc = launch_dt_from_max(cs, c->dt_d, cfl, c->dtv_d))) break;
+    }
     if ((rc = stx_advance_solution(c, cs, f, dt, 0.0))) break;
     if ((rc = stx_compute_aux(c, cs, f->w, f->w_aux, 1, 0))) break;
-    k_time_add<<<1, 1, 0, cs>>>(c->time_d, dt);
-    if (cudaGetLastError() != cudaSuccess) rc = STX_E_CUDA;
+    if (dev) {
+      if ((rc = launch_time_advance(cs, c->time_d, c->dtv_d))) break;
+    } else {
+      k_time_add<<<1, 1, 0, cs>>>(c->time_d, dt);
+      if (cudaGetLastError() != cudaSuccess) rc = STX_E_CUDA;
+    }
   }
   if (e == cudaSuccess) {
     cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
     if (e2 != cudaSuccess && rc == STX_OK) rc = STX_E_CUDA;
   }
   c->d.p.time_d = nullptr;
+  c->d.p.dt_d = nullptr;
   c->prof_on = prof;
   stx_graph *g = nullptr;
   if (rc == STX_OK) {
@@ -881,10 +922,22 @@ int stx_graph_create(stx_ctx *c, const stx_fields *f, double dt, int nsteps, stx
     return rc;
   }
   g->c = c;
-  g->dt = dt;
+  g->dt = dev ? 0.0 : dt;
+  g->cfl = dev ? cfl : 0.0;
   g->nsteps = nsteps;
   *out = g;
   return STX_OK;
+}
+}  // namespace
+
+int stx_graph_create(stx_ctx *c, const stx_fields *f, double dt, int nsteps, stx_graph **out) {
+  if (!c || !f || !out || nsteps < 1 || !(dt > 0.0)) return STX_E_INVALID;
+  return graph_create_impl(c, f, dt, 0.0, nsteps, out);
+}
+
+int stx_graph_create_cfl(stx_ctx *c, const stx_fields *f, double cfl, int nsteps, stx_graph **out) {
+  if (!c || !f || !out || nsteps < 1 || !(cfl > 0.0)) return STX_E_INVALID;
+  return graph_create_impl(c, f, 0.0, cfl, nsteps, out);
 }
 
 int stx_graph_launch(stx_graph *g, void *s, double time) {
@@ -892,6 +945,16 @@ int stx_graph_launch(stx_graph *g, void *s, double time) {
   k_time_set<<<1, 1, 0, S(s)>>>(g->c->time_d, time);
   STX_CUDA_TRY(cudaGetLastError());
   STX_CUDA_TRY(cudaGraphLaunch(g->exec, S(s)));
+  return STX_OK;
+}
+
+int stx_graph_state(stx_graph *g, void *s, double *time, double *dt) {
+  if (!g || !time || !dt) return STX_E_INVALID;
+  double h[2];
+  STX_CUDA_TRY(cudaMemcpyAsync(h, g->c->time_d, sizeof(h), cudaMemcpyDeviceToHost, S(s)));
+  STX_CUDA_TRY(cudaStreamSynchronize(S(s)));
+  *time = h[0];
+  *dt = g->dt > 0.0 ? g->dt : h[1];
   return STX_OK;
 }
 

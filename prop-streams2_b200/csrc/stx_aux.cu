@@ -549,8 +549,11 @@ __global__ void k_bc_nr(DevCtx c, const double *__restrict__ wa, const double *_
 // ============================================================== RK bookkeeping
 // init_flux_cuf / init_flux_simpler_cuf / update_flux_cuf / update_simpler_flux_cuf
 // (kernels_gpu.F90:28-66, 3297-3334); fl is (nx,ny,nz,nv) so these are flat maps.
+// dt_d (captured CFL-driven steps): rhodt / gamdt hold the RK coefficient, and
+// the scalar is coefficient * (scale * dt) with dt from device memory
 __global__ void k_init_flux(double *__restrict__ fl, double *__restrict__ fln, const double *__restrict__ fl_sav,
-                            double rhodt, long long n) {
+                            double rhodt, long long n, const double *__restrict__ dt_d, double scale) {
+  if (dt_d) rhodt = rhodt * (scale * *dt_d);
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   for (; q < n; q += (long long)gridDim.x * blockDim.x) {
     double f = fl[q];
@@ -559,7 +562,8 @@ __global__ void k_init_flux(double *__restrict__ fl, double *__restrict__ fln, c
   }
 }
 __global__ void k_update_flux(const double *__restrict__ fl, double *__restrict__ fln, const double *__restrict__ fl_sav,
-                              double gamdt, long long n) {
+                              double gamdt, long long n, const double *__restrict__ dt_d, double scale) {
+  if (dt_d) gamdt = gamdt * (scale * *dt_d);
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   for (; q < n; q += (long long)gridDim.x * blockDim.x)
     fln[q] = fl_sav ? fln[q] - gamdt * (fl[q] - fl_sav[q]) : fln[q] - gamdt * fl[q];
@@ -572,8 +576,9 @@ __global__ void k_copy(const double *__restrict__ a, double *__restrict__ b, lon
 // update_flux: fln -= gamdt*fl (or gamdt*(fl - fl_sav)); w += fln where fluid.
 __global__ void k_update_field(DevCtx c, double *__restrict__ w, const double *__restrict__ fl, double *__restrict__ fln,
                                const double *__restrict__ fl_sav, const int32_t *__restrict__ mask, double gamdt,
-                               int fused, int nv) {
+                               int fused, int nv, double scale) {
   const DevGrid &g = c.g;
+  if (c.p.dt_d) gamdt = gamdt * (scale * *c.p.dt_d);
   long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= g.npi) return;
   int i = 1 + (int)(tid % g.nx);
@@ -783,20 +788,22 @@ int launch_bc_nr(const DevCtx &c, cudaStream_t s, const double *wa, const double
   return STX_OK;
 }
 
-int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt) {
+int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt,
+                     double scale) {
   long long n = c.g.npi * (c.t.ns + 4);
   int nb = grid1d(n, 256);
   if (nb > 148 * 32) nb = 148 * 32;
-  k_init_flux<<<nb, 256, 0, s>>>(fl, fln, fl_sav, rhodt, n);
+  k_init_flux<<<nb, 256, 0, s>>>(fl, fln, fl_sav, rhodt, n, c.p.dt_d, scale);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
 
-int launch_update_flux(const DevCtx &c, cudaStream_t s, const double *fl, double *fln, const double *fl_sav, double gamdt) {
+int launch_update_flux(const DevCtx &c, cudaStream_t s, const double *fl, double *fln, const double *fl_sav, double gamdt,
+                       double scale) {
   long long n = c.g.npi * (c.t.ns + 4);
   int nb = grid1d(n, 256);
   if (nb > 148 * 32) nb = 148 * 32;
-  k_update_flux<<<nb, 256, 0, s>>>(fl, fln, fl_sav, gamdt, n);
+  k_update_flux<<<nb, 256, 0, s>>>(fl, fln, fl_sav, gamdt, n, c.p.dt_d, scale);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
@@ -811,8 +818,29 @@ int launch_copy(const DevCtx &c, cudaStream_t s, const double *a, double *b) {
 }
 
 int launch_update_field(const DevCtx &c, cudaStream_t s, double *w, const double *fl, double *fln, const double *fl_sav,
-                        const int32_t *mask, double gamdt, int fused) {
-  k_update_field<<<grid1d(c.g.npi, 256), 256, 0, s>>>(c, w, fl, fln, fl_sav, mask, gamdt, fused, c.t.ns + 4);
+                        const int32_t *mask, double gamdt, int fused, double scale) {
+  k_update_field<<<grid1d(c.g.npi, 256), 256, 0, s>>>(c, w, fl, fln, fl_sav, mask, gamdt, fused, c.t.ns + 4, scale);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+
+__global__ void k_dt_from_max(const unsigned long long *__restrict__ max9, double cfl, double *__restrict__ dt) {
+  double m = __longlong_as_double((long long)max9[0]);
+  for (int q = 1; q < 9; q++) {
+    const double v = __longlong_as_double((long long)max9[q]);
+    if (v > m) m = v;
+  }
+  *dt = cfl / m;
+}
+__global__ void k_time_advance(double *__restrict__ t, const double *__restrict__ dt) { *t = *t + *dt; }
+
+int launch_dt_from_max(cudaStream_t s, const unsigned long long *max9, double cfl, double *dt) {
+  k_dt_from_max<<<1, 1, 0, s>>>(max9, cfl, dt);
+  STX_CUDA_TRY(cudaGetLastError());
+  return STX_OK;
+}
+int launch_time_advance(cudaStream_t s, double *t, const double *dt) {
+  k_time_advance<<<1, 1, 0, s>>>(t, dt);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }

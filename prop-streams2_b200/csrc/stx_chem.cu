@@ -30,6 +30,7 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
   const DevGrid &g = c.g;
   const int NV = NS + 4;
   const double eps_Z = 5e-4;
+  if (c.p.dt_d) dttry = dttry * *c.p.dt_d;   // captured CFL-driven step: dttry holds the splitting's factor
   if (c.p.time_d) {                 // captured step: the window starts at the device-held time
     t0 = *c.p.time_d;
     t1 = t0 + dttry;
@@ -274,6 +275,7 @@ __global__ void __launch_bounds__(chem_block(NS)) k_rosenbrock(DevCtx c, double 
                                                     double dttry, double t0, double t1, unsigned int *counter) {
   const DevGrid &g = c.g;
   const int NV = NS + 4;
+  if (c.p.dt_d) dttry = dttry * *c.p.dt_d;   // captured CFL-driven step: dttry holds the splitting's factor
   if (c.p.time_d) {                 // captured step: the window starts at the device-held time
     t0 = *c.p.time_d;
     t1 = t0 + dttry;

@@ -77,6 +77,13 @@ struct DevPar {
   // from it (the same double operations the host performs) instead of their
   // t0 / t1 arguments, so a replayed step sees the current time.
   const double *time_d;
+  // Step size in device memory, set only while a CFL-driven step is captured
+  // (stx_graph_create_cfl; its last computation in the step, from the CFL
+  // maxima): a kernel that takes a dt-derived scalar by value (rhodt, gamdt,
+  // the chemistry's dttry) then receives its coefficient in that argument and
+  // forms coefficient * (scale * dt), the double operations the host performs
+  // on its own dt (scale: the factor of the splitting, 1 or 0.5).
+  const double *dt_d;
   // precision form: 0 plain FP64; 1 mixed -- central face fluxes, viscous and
   // diffusive fluxes and the transport properties in FP32 (RK residual still
   // accumulated in FP64; T(e) Newton, rates, K_c and the chemistry in FP64)

@@ -678,15 +678,20 @@ template <int NS, int DIR, bool TMA = false> struct ETile {
   static constexpr int NP = TC + 3;                    // pair origins per line and distance
   static constexpr int NVC = NS + 7;                   // staged fields
   static constexpr int NT = TC * NL;                   // threads
-  // staged cells of the x sweep's TMA copies: a row of BX cells from an even x
-  // (16-byte rule of tensor copies), landing at a 128-byte-aligned row of RS cells
+  // the cell stage of tensor copies (TMA), whose boxes start at an even x (the
+  // 16-byte rule of tensor copies) and land at 128-byte-aligned addresses:
+  //   x: per field and line a row of BX = S + 2 cells, at a row stride RS;
+  //   y / z: per field a box of S sweep cells x BXI = NL + 2 cells in i (row
+  //   stride RSI), the fields VS apart
   static constexpr int BX = S + 2;
-  static constexpr int RS = TMA ? ((BX * 8 + 127) / 128) * 16 : S;   // row stride of the cell stage
-  static constexpr int VS = DIR == 0 ? NL * RS : S * NL;             // field stride of the cell stage
+  static constexpr int BXI = NL + 2;
+  static constexpr int RS = TMA ? ((BX * 8 + 127) / 128) * 16 : S;   // x: row stride of the cell stage
+  static constexpr int RSI = TMA ? BXI : NL;                         // y / z: row stride of the cell stage
+  static constexpr int VS = DIR == 0 ? NL * RS : (TMA ? ((S * BXI * 8 + 127) / 128) * 16 : S * NL);
   // x sweep: the sweep is the contiguous direction, lines are rows (j, k);
   // y / z sweeps: lines are consecutive i
   __device__ static int sx(int s, int l) { return DIR == 0 ? l * S + s : s * NL + l; }     // per-cell arrays
-  __device__ static int cx(int s, int l) { return DIR == 0 ? l * RS + s : s * NL + l; }    // the cell stage
+  __device__ static int cx(int s, int l) { return DIR == 0 ? l * RS + s : s * RSI + l; }   // the cell stage
   __device__ static int px(int a, int l) { return DIR == 0 ? l * NP + a : a * NL + l; }
   __device__ static int fx(int f, int l) { return DIR == 0 ? l * NF + f : f * NL + l; }
 };
@@ -699,7 +704,7 @@ __host__ __device__ constexpr size_t etile_smem(int dir) {
                         (size_t)(NS + 4) * ETile<NS, 0>::NF * ETile<NS, 0>::NL * sizeof(R) +
                         (size_t)6 * ETile<NS, 0>::NP * ETile<NS, 0>::NL * sizeof(R) +
                         (size_t)ETile<NS, 0>::S * ETile<NS, 0>::NL * sizeof(R)
-                  : (size_t)ETile<NS, 1>::NVC * ETile<NS, 1>::S * ETile<NS, 1>::NL * 8 +
+                  : (size_t)ETile<NS, 1, TMA>::NVC * ETile<NS, 1, TMA>::VS * 8 + (TMA ? 128 : 0) +
                         (size_t)(NS + 4) * ETile<NS, 1>::NF * ETile<NS, 1>::NL * sizeof(R) +
                         (size_t)6 * ETile<NS, 1>::NP * ETile<NS, 1>::NL * sizeof(R) +
                         (size_t)ETile<NS, 1>::S * ETile<NS, 1>::NL * sizeof(R);
@@ -736,6 +741,14 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
       ::"r"(smem_u32(dst)), "l"((unsigned long long)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
+// 4-D tile load of the box at (x, y, z, w) of the tensor map into dst, completing on bar
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
+                                            int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
+      ::"r"(smem_u32(dst)), "l"((unsigned long long)map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "r"(w)
+      : "memory");
+}
 // bounded wait for phase `phase` of bar: false if it did not complete within the limit
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t phase) {
   for (int it = 0; it < (1 << 22); it++)
@@ -758,11 +771,11 @@ __device__ __forceinline__ int etile_field(int v) {
   }
 }
 
-// TMA (x sweep only): the cell stage is filled by 2-D tensor copies of the
-// staged rows (tmap: w_aux as nxg x (nyg nzg nv_aux) doubles), issued by one
-// thread and completed on an mbarrier; cells outside the ghosted box come back
-// as zeros (the copies' out-of-bounds fill), as the loads of the plain staging
-// give them.  Everything after the staging is the same code on the same values.
+// TMA: the cell stage is filled by tensor copies (tmap: sweep_tmap) -- per
+// staged row in x, per field in y / z -- issued by one thread and completed on
+// an mbarrier; cells outside the ghosted box come back as zeros (the copies'
+// out-of-bounds fill), as the loads of the plain staging give them.
+// Everything after the staging is the same code on the same values.
 template <int NS, int DIR, typename R, bool TMA = false>
 __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MINB : 2)
     k_euler_tile(DevCtx c, const DevCtx *__restrict__ cg, const double *__restrict__ wa, double *__restrict__ fl,
@@ -829,27 +842,45 @@ __global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MIN
   // 1. stage the cells c0-3 .. c0+TC+2 of every line (zero outside the ghosted box)
   const double *scb = sc;                                 // staged cell 0 of field 0, line 0
   if constexpr (TMA) {
-    static_assert(DIR == 0, "tensor-copy staging is built for the x sweep");
-    const int xs = c0 - T::H + g.ng - 1;                  // ghosted x index (0-based) of staged cell 0
-    const int x0 = xs & ~1;                               // an even x: 16 bytes of doubles
-    scb = sc + (xs - x0);
-    if (t == 0) {
-      int nact = 0;
-      for (int l = 0; l < NL; l++) nact += s_gb[l] >= 0;
-      fence_proxy_async();                                // the previous reads of this stage come first
-      mbar_expect_tx(&s_bar, (uint32_t)(nact * NVC * T::BX * 8));
-      const long long rows = (long long)g.nyg * g.nzg;
-      for (int l = 0; l < NL; l++) {
-        const long long gb = s_gb[l];
-        if (gb < 0) continue;
-        const long long line = (gb - (g.ng - 1)) / g.nxg;   // (j + ng - 1) + nyg (k + ng - 1)
+    if constexpr (DIR == 0) {
+      const int xs = c0 - T::H + g.ng - 1;                // ghosted x index (0-based) of staged cell 0
+      const int x0 = xs & ~1;                             // an even x: 16 bytes of doubles
+      scb = sc + (xs - x0);
+      if (t == 0) {
+        int nact = 0;
+        for (int l = 0; l < NL; l++) nact += s_gb[l] >= 0;
+        fence_proxy_async();                              // the previous reads of this stage come first
+        mbar_expect_tx(&s_bar, (uint32_t)(nact * NVC * T::BX * 8));
+        const long long rows = (long long)g.nyg * g.nzg;
+        for (int l = 0; l < NL; l++) {
+          const long long gb = s_gb[l];
+          if (gb < 0) continue;
+          const long long line = (gb - (g.ng - 1)) / g.nxg;   // (j + ng - 1) + nyg (k + ng - 1)
+          for (int v = 0; v < NVC; v++)
+            tma_load_2d(sc + v * T::VS + l * T::RS, &tmap, &s_bar, x0,
+                        (int)((etile_field<NS>(v) - 1) * rows + line));
+        }
+      }
+      for (int e = t; e < NVC * T::VS; e += NT)           // lines outside the grid: zeros
+        if (s_gb[(e / T::RS) % NL] < 0) sc[e] = 0.0;
+    } else {
+      // one box per field: BXI cells in i from an even x by S cells along the
+      // sweep (tmap: w_aux as nxg x nyg x nzg x nv_aux); lines past nx stage
+      // whatever lies there (the ghosts, or the copies' zero fill) and are
+      // never used
+      const int xg = blockIdx.x * NL + g.ng;              // ghosted i index (0-based) of line 0
+      const int x0 = xg & ~1;
+      scb = sc + (xg - x0);
+      if (t == 0) {
+        fence_proxy_async();
+        mbar_expect_tx(&s_bar, (uint32_t)(NVC * T::BXI * S * 8));
+        const int ss = c0 - T::H + g.ng - 1;              // ghosted sweep index of staged cell 0
+        const int o = blockIdx.z + g.ng;                  // ghosted index of the other lateral direction
         for (int v = 0; v < NVC; v++)
-          tma_load_2d(sc + v * T::VS + l * T::RS, &tmap, &s_bar, x0,
-                      (int)((etile_field<NS>(v) - 1) * rows + line));
+          tma_load_4d(sc + v * T::VS, &tmap, &s_bar, x0, DIR == 1 ? ss : o, DIR == 1 ? o : ss,
+                      etile_field<NS>(v) - 1);
       }
     }
-    for (int e = t; e < NVC * T::VS; e += NT)             // lines outside the grid: zeros
-      if (s_gb[(e / T::RS) % NL] < 0) sc[e] = 0.0;
     // every thread waits for the copies (bounded); on a time-out the CTA stops
     // together and the status word says so
     const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0));
@@ -1122,18 +1153,22 @@ long long weno_scratch_faces(const DevGrid &g) {
   return m > d ? m : d;
 }
 
-// The x sweep's tensor map over w_aux (2-D: nxg doubles per row, nyg nzg nv_aux
-// rows; box: one staged row of ETile::BX doubles), encoded through the driver's
-// entry point and cached per (pointer, grid).  No map -- false -- when the
-// layout breaks a rule of tensor copies (a row stride that is not a multiple of
-// 16 bytes, i.e. odd nxg; a base that is not 16-byte aligned; more rows than a
-// 32-bit coordinate) or the entry point is missing: the sweep then stages with
-// plain loads.  STX_TMA=0 turns the tensor copies off.
-static bool xsweep_tmap(const DevGrid &g, int nv_aux, const double *wa, CUtensorMap *out) {
+// The staged sweeps' tensor maps over w_aux, encoded through the driver's
+// entry point and cached per (pointer, grid, direction):
+//   x: 2-D, nxg doubles per row, nyg nzg nv_aux rows; box: one staged row of
+//      ETile::BX doubles;
+//   y / z: 4-D, nxg x nyg x nzg x nv_aux; box: ETile::BXI doubles in i by
+//      ETile::S cells along the sweep (one field).
+// No map -- false -- when the layout breaks a rule of tensor copies (a row
+// stride that is not a multiple of 16 bytes, i.e. odd nxg; a base that is not
+// 16-byte aligned; more rows than a 32-bit coordinate) or the entry point is
+// missing: the sweep then stages with plain loads.  STX_TMA=0 turns the tensor
+// copies off.
+static bool sweep_tmap(int dir, const DevGrid &g, int nv_aux, const double *wa, CUtensorMap *out) {
   static std::mutex mu;
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   static bool tried = false, off = false;
-  static std::map<std::tuple<uintptr_t, int, int, int, int>, CUtensorMap> cache;
+  static std::map<std::tuple<uintptr_t, int, int, int, int, int>, CUtensorMap> cache;
   const long long rows = (long long)g.nyg * g.nzg * nv_aux;
   if ((g.nxg & 1) || (((uintptr_t)wa) & 15) || rows >= 0x7fffffffLL) return false;
   std::lock_guard<std::mutex> lk(mu);
@@ -1148,21 +1183,34 @@ static bool xsweep_tmap(const DevGrid &g, int nv_aux, const double *wa, CUtensor
       encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
   }
   if (off || !encode) return false;
-  auto key = std::make_tuple((uintptr_t)wa, g.nxg, g.nyg, g.nzg, nv_aux);
+  auto key = std::make_tuple((uintptr_t)wa, g.nxg, g.nyg, g.nzg, nv_aux, dir);
   auto it = cache.find(key);
   if (it != cache.end()) {
     *out = it->second;
     return true;
   }
   CUtensorMap m;
-  const cuuint64_t dims[2] = {(cuuint64_t)g.nxg, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)g.nxg * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)ETile<9, 0, true>::BX, 1};
-  const cuuint32_t estr[2] = {1, 1};
-  if (encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)wa, dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return false;
+  CUresult r;
+  if (dir == 0) {
+    const cuuint64_t dims[2] = {(cuuint64_t)g.nxg, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)g.nxg * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)ETile<9, 0, true>::BX, 1};
+    const cuuint32_t estr[2] = {1, 1};
+    r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)wa, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  } else {
+    const cuuint64_t dims[4] = {(cuuint64_t)g.nxg, (cuuint64_t)g.nyg, (cuuint64_t)g.nzg, (cuuint64_t)nv_aux};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.nxg * sizeof(double), (cuuint64_t)g.nxg * g.nyg * sizeof(double),
+                                   (cuuint64_t)g.npg * sizeof(double)};
+    const cuuint32_t bi = (cuuint32_t)ETile<9, 1, true>::BXI, bs = (cuuint32_t)ETile<9, 1, true>::S;
+    const cuuint32_t box[4] = {bi, dir == 1 ? bs : 1u, dir == 1 ? 1u : bs, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)wa, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  }
+  if (r != CUDA_SUCCESS) return false;
   if (cache.size() > 64) cache.clear();
   cache[key] = m;
   *out = m;
@@ -1203,15 +1251,11 @@ static int euler_tile_launch(const DevCtx &c, const DevCtx *cg, cudaStream_t s, 
   dim3 grid((unsigned)lgrp, (unsigned)tiles, (unsigned)other);
   CUtensorMap tm;
   std::memset(&tm, 0, sizeof(tm));
-  bool tma = false;
-  if constexpr (DIR == 0) {
-    if (xsweep_tmap(g, c.p.nv_aux, wa, &tm)) {
-      tma = true;
-      k_euler_tile<NS, 0, R, true><<<grid, T::NT, etile_smem<NS, R, true>(0), s>>>(c, cg, wa, fl, nmin, nmax, ow,
-                                                                                   fhw, cap, tm);
-    }
-  }
-  if (!tma) k_euler_tile<NS, DIR, R><<<grid, T::NT, smem, s>>>(c, cg, wa, fl, nmin, nmax, ow, fhw, cap, tm);
+  if (sweep_tmap(DIR, g, c.p.nv_aux, wa, &tm))
+    k_euler_tile<NS, DIR, R, true><<<grid, T::NT, etile_smem<NS, R, true>(DIR), s>>>(c, cg, wa, fl, nmin, nmax, ow,
+                                                                                     fhw, cap, tm);
+  else
+    k_euler_tile<NS, DIR, R><<<grid, T::NT, smem, s>>>(c, cg, wa, fl, nmin, nmax, ow, fhw, cap, tm);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }
@@ -1276,6 +1320,14 @@ static int euler_setup_t() {
                                       (int)etile_smem<NS, float>(1)));
     STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)etile_smem<NS, float>(2)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 1, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, double, true>(1)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 2, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, double, true>(2)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 1, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, float, true>(1)));
+    STX_CUDA_TRY(cudaFuncSetAttribute(k_euler_tile<NS, 2, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)etile_smem<NS, float, true>(2)));
   }
   return STX_OK;
 }

@@ -12,11 +12,20 @@ int launch_bc_face_thermo(const DevCtx &c, cudaStream_t s, double *w, double *wa
 // characteristic boundary treatment of face ilat (bc_nr_lat_*), added to fl
 int launch_bc_nr(const DevCtx &c, cudaStream_t s, const double *wa, const double *w, double *fl, const double *winf,
                  int ilat, int nr_type);
-int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt);
-int launch_update_flux(const DevCtx &c, cudaStream_t s, const double *fl, double *fln, const double *fl_sav, double gamdt);
+// scale: with c.p.dt_d set (captured CFL-driven steps), rhodt / gamdt are the RK
+// coefficient and the kernels form coefficient * (scale * dt) from the device dt
+int launch_init_flux(const DevCtx &c, cudaStream_t s, double *fl, double *fln, const double *fl_sav, double rhodt,
+                     double scale = 1.0);
+int launch_update_flux(const DevCtx &c, cudaStream_t s, const double *fl, double *fln, const double *fl_sav, double gamdt,
+                       double scale = 1.0);
 int launch_copy(const DevCtx &c, cudaStream_t s, const double *a, double *b);
 int launch_update_field(const DevCtx &c, cudaStream_t s, double *w, const double *fl, double *fln, const double *fl_sav,
-                        const int32_t *mask, double gamdt, int fused);
+                        const int32_t *mask, double gamdt, int fused, double scale = 1.0);
+// the step size from the nine CFL maxima (bit patterns, as k_compute_dt leaves
+// them): *dt = cfl / max, the host's operations
+int launch_dt_from_max(cudaStream_t s, const unsigned long long *max9, double cfl, double *dt);
+// *t = *t + *dt (the time advance of a captured CFL-driven step)
+int launch_time_advance(cudaStream_t s, double *t, const double *dt);
 int launch_compute_dt(const DevCtx &c, cudaStream_t s, const double *wa, const int32_t *mask, unsigned long long *out9);
 // compute_residual + rho/T/p extrema: STX_RES_BLOCKS partial sums in part, 6 extrema in mm
 #define STX_RES_BLOCKS 296

@@ -122,7 +122,9 @@ STX_SIGNATURES = [
     ("stx_batch0d_integrate", _I, [_VP, _VP, _I, _VP, _VP, _VP, _D, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP]),
     ("stx_set_precision", _I, [_VP, _I]),
     ("stx_graph_create", _I, [_VP, C.POINTER(StxFields), _D, _I, C.POINTER(_VP)]),
+    ("stx_graph_create_cfl", _I, [_VP, C.POINTER(StxFields), _D, _I, C.POINTER(_VP)]),
     ("stx_graph_launch", _I, [_VP, _VP, _D]),
+    ("stx_graph_state", _I, [_VP, _VP, C.POINTER(_D), C.POINTER(_D)]),
     ("stx_graph_destroy", _I, [_VP]),
     ("stx_rk_sync", _I, [_VP, _VP, C.POINTER(StxFields), _D, _I]),
     ("stx_advance_solution", _I, [_VP, _VP, C.POINTER(StxFields), _D, _D]),

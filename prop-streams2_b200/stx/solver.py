@@ -105,25 +105,38 @@ class Solver:
     # ------------------------------------------------------------------ captured steps
     def capture(self, nsteps: int):
         """Capture nsteps iterations of the integration loop into one CUDA graph
-        (fixed dt only: cfl < 0, iter_dt_recompute = 1).  Replaying it with
-        ``replay`` gives the same result as nsteps calls of ``step``."""
-        if self.case.cfl >= 0 or self.case.iter_dt_recompute != 1:
-            raise ValueError("captured steps need a fixed dt (cfl < 0) and iter_dt_recompute = 1")
-        self.dt = -self.case.cfl
+        (iter_dt_recompute = 1).  Fixed dt (cfl < 0): the step size is known; a
+        CFL-driven run (cfl > 0): every captured step forms its dt from the CFL
+        maxima on the device.  Replaying it with ``replay`` gives the same result
+        as nsteps calls of ``step``."""
+        if self.case.iter_dt_recompute != 1:
+            raise ValueError("captured steps need iter_dt_recompute = 1")
         g = C.c_void_p()
-        check(self.lib.stx_graph_create(self.ctx, C.byref(self.fields), self.dt, nsteps, C.byref(g)),
-              "stx_graph_create")
+        if self.case.cfl < 0:
+            self.dt = -self.case.cfl
+            check(self.lib.stx_graph_create(self.ctx, C.byref(self.fields), self.dt, nsteps, C.byref(g)),
+                  "stx_graph_create")
+        else:
+            check(self.lib.stx_graph_create_cfl(self.ctx, C.byref(self.fields), self.case.cfl, nsteps, C.byref(g)),
+                  "stx_graph_create_cfl")
         if not hasattr(self, "_graphs"):
             self._graphs = []
         self._graphs.append(g)
         return g, nsteps
 
     def replay(self, graph):
+        """Launch a captured graph.  A CFL-driven graph's time and last dt are
+        read back (one synchronisation per replay)."""
         g, n = graph
         check(self.lib.stx_graph_launch(g, self.stream, self.time), "stx_graph_launch")
-        for _ in range(n):
-            self.icyc += 1
-            self.time = self.time + self.dt
+        self.icyc += n
+        if self.case.cfl < 0:
+            for _ in range(n):
+                self.time = self.time + self.dt
+        else:
+            t, dt = C.c_double(), C.c_double()
+            check(self.lib.stx_graph_state(g, self.stream, C.byref(t), C.byref(dt)), "stx_graph_state")
+            self.time, self.dt = t.value, dt.value
 
     def __del__(self):
         try:

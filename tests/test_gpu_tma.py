@@ -1,10 +1,11 @@
-"""The x sweep's tensor-copy staging (cp.async.bulk.tensor into shared memory,
-completed on an mbarrier) against the plain staging loads: the same staged
-values, so the same fluxes and cell updates bit for bit.  STX_TMA=0 (read once
-per process) selects the plain loads, so each arm runs in its own process.
-Cases: a developed turbulence field (hybrid central / listed WENO faces), an
-all-WENO field, and a sweep starting at cell 2 (a characteristic boundary at
-xmin), whose staged rows start at an odd x and land one cell into the row."""
+"""The staged sweeps' tensor-copy staging (cp.async.bulk.tensor into shared
+memory, completed on an mbarrier) against the plain staging loads, in x, y and
+z: the same staged values, so the same fluxes and cell updates bit for bit.
+STX_TMA=0 (read once per process) selects the plain loads, so each arm runs in
+its own process.  Cases: a developed turbulence field (hybrid central / listed
+WENO faces), an all-WENO field on a grid whose sizes are not multiples of the
+tiles, and sweeps starting at cell 2 (characteristic boundaries), whose staged
+x rows start at an odd x and land one cell into the row."""
 import os
 import subprocess
 import sys
@@ -33,11 +34,11 @@ if case_kind == "turb":
     s = Solver(case, w=torch.from_numpy(W).cuda(), w_aux=torch.from_numpy(WA).cuda())
     nmin = 1
 elif case_kind == "weno":
-    case = H.synthetic_case(n=(150, 10, 9), seed=3, sensor_threshold=-1.0)
+    case = H.synthetic_case(n=(150, 37, 21), seed=3, sensor_threshold=-1.0)
     s = Solver(case)
     nmin = 1
 else:
-    case = H.synthetic_case(n=(150, 10, 9), seed=3, bc=(2, 2, 0, 0, 0, 0), bc_nr=(1, 1, 0, 0, 0, 0),
+    case = H.synthetic_case(n=(150, 30, 20), seed=3, bc=(2, 2, 2, 2, 2, 2), bc_nr=(1, 1, 1, 1, 1, 1),
                             sensor_threshold=0.02, sensor_type=0)
     s = Solver(case)
     nmin = 2
@@ -45,14 +46,19 @@ s.prepare()
 for _ in range(2 if case_kind == "turb" else 0):
     s.step()
 s.compute_aux(1, 1)
-fl = torch.zeros_like(s.fl)
 stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-rc = s.lib.stx_euler_x(s.ctx, stream, C.c_void_p(s.w_aux.data_ptr()), C.c_void_p(fl.data_ptr()), nmin,
-                       case.nx - (nmin - 1), 1)
-assert rc == 0, rc
+res = []
+for name, n in (("x", case.nx), ("y", case.ny), ("z", case.nz)):
+    for prec in (0, 1):
+        s.lib.stx_set_precision(s.ctx, prec)
+        fl = torch.zeros_like(s.fl)
+        rc = getattr(s.lib, "stx_euler_" + name)(s.ctx, stream, C.c_void_p(s.w_aux.data_ptr()),
+                                                C.c_void_p(fl.data_ptr()), nmin, n - (nmin - 1), 1)
+        assert rc == 0, rc
+        res.append(fl.cpu().numpy())
 torch.cuda.synchronize()
 assert s.status(reset=False) & 0x10 == 0          # no tensor-copy wait timed out
-np.save(out, fl.cpu().numpy())
+np.save(out, np.stack(res))
 '''
 
 
