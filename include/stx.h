@@ -130,7 +130,8 @@ const char *stx_strerror(int code);
 int stx_ctx_create(const stx_params *par, const stx_tables *tab, const stx_grid *grid, stx_ctx **out);
 /* A context for another grid and parameter set on the same mechanism: it uses
  * base's device tables (no table upload or repacking) and has its own grid,
- * scratch, counters and status word.  base must outlive every context created
+ * scratch, counters and status word; it starts in base's precision form
+ * (stx_set_precision).  base must outlive every context created
  * from it.  No counterpart in the reference (one solve per process); for
  * callers that run many solves of one mechanism, e.g. a request server. */
 int stx_ctx_create_like(const stx_ctx *base, const stx_params *par, const stx_grid *grid, stx_ctx **out);
@@ -312,8 +313,8 @@ int stx_batch0d_integrate(stx_ctx *ctx, void *stream, int n, const double *T0, c
  * So that no call allocates, a call whose kernel needs more than the current
  * limit launches nothing and returns STX_E_LOCAL_MEM.  Raise the limit once at
  * initialisation, e.g. cudaDeviceSetLimit(cudaLimitStackSize, 4608) for up to
- * 14 species or 12288 for 53 (this build's frames: 3168 B at 9 species, 3904 B
- * at 14, 10528 B at 53; the call checks the kernel's actual figure). */
+ * 14 species or 12288 for 53 (this build's frames: 2704 B at 9 species, 3488 B
+ * at 14, 10432 B at 53; the call checks the kernel's actual figure). */
 int stx_rosenbrock_krylov_noalloc(const stx_params *par, const stx_tables *tab_dev, const stx_grid *grid,
                                   void *stream, double *w, const double *w_aux, const double *fl_sav,
                                   double dttry, double time_start, double time_end, int simpler, uint32_t *status);

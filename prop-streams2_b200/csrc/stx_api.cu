@@ -439,6 +439,7 @@ static int ctx_create_impl(const stx_params *par, const stx_tables *tab, const s
   c->time_d = (double *)tm;
   c->dtv_d = (double *)tm + 1;
   p.status = c->status_d;
+  if (base) p.mixed = base->d.p.mixed;   // a context like base takes its precision form
   {
     const char *ek = std::getenv("STX_EULER_KERNEL");
     int face = ek && std::strcmp(ek, "face") == 0;

@@ -183,7 +183,10 @@ class Server:
     (graphs: as one replay of a captured graph of chunk steps);
     reactor_batch: most reactors per batched launch (the default, 1024, stays
     within the reactors the warp-per-reactor kernel runs at once on a B200, so
-    every served batch, like a request served alone, takes that kernel)."""
+    every served batch, like a request served alone, takes that kernel).
+    precision: the grid solves' form, "fp64" (the reference method) or "mixed"
+    (FP32 face fluxes and transport, stx_set_precision); the reactors' chemistry
+    is FP64 in both."""
 
     # torch hands out the streams of a per-device pool of 32 in turn; the
     # lanes' and the grid solves' streams must all be distinct
@@ -191,7 +194,7 @@ class Server:
 
     def __init__(self, device: str = "cuda", mem_budget: int = 16 << 30, max_grid: int = 20, chunk: int = 5,
                  reactor_batch: int = 1024, t_max: float = 1e-2, max_steps: int = 20000, reactor_lanes: int = 12,
-                 graphs: bool = True):
+                 graphs: bool = True, precision: str = "fp64"):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -234,6 +237,10 @@ class Server:
                               device=str(self.device)),
             "tube2d": Solver(configs.tube_case(16, 4, tables=self.tables["tube2d"]), device=str(self.device)),
         }
+        # every request's context takes its base's precision form (stx_ctx_create_like_on)
+        self.precision = precision
+        for b in self._bases.values():
+            b.set_precision(precision)
         # host time of every call site of the loop: name -> [calls, total s, max s]
         self.trace: Dict[str, list] = {}
 

@@ -62,7 +62,13 @@ def slab_case(k0, k1):
     ng = c.ng
     c.w[:] = full.w[:, k0 - 1:k1 + 2 * ng, :, :]
     c.w_aux[:] = full.w_aux[:, k0 - 1:k1 + 2 * ng, :, :]
-    assert np.allclose(c.dzitdz, full.dzitdz[:c.nz])
+    # the whole box's z coordinates and metrics of these planes: a slab's own
+    # grid starts at z = 0, and its finite-difference metrics then round
+    # differently from the box's in the last bit
+    assert np.allclose(c.dzitdz, full.dzitdz[k0 - 1:k1])
+    c.z[:] = full.z[k0 - 1:k1 + 2 * ng]
+    c.dzitdz[:] = full.dzitdz[k0 - 1:k1]
+    c.dzitdzs[:] = full.dzitdzs[k0 - 1:k1]
     return D.make_z_slab(c)
 
 
