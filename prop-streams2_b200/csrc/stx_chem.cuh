@@ -310,6 +310,20 @@ static __device__ void inv_matrix_k(double *a, int d) {
 #undef AK
 }
 
+// The ROK4 method's coefficients (rosenbrock_krylov_kernel, kernels_gpu.F90:10463-10480),
+// in constant memory: indexed by the rolled stage loops, a per-thread copy
+// takes 256 bytes of every thread's local frame.
+__constant__ double c_rok4_alpha[STX_NSTAGE][3] = {{0.0, 0.0, 0.0},
+                                                   {0.432364435748567, 0.0, 0.0},
+                                                   {-0.514211316876170, 1.382271144617360, 0.0},
+                                                   {-0.514211316876170, 1.382271144617360, 0.0}};
+__constant__ double c_rok4_gmc[STX_NSTAGE][3] = {{0.0, 0.0, 0.0},
+                                                 {-0.602765307997356, 0.0, 0.0},
+                                                 {-1.389195789724843, 1.072950969011413, 0.0},
+                                                 {0.992356412977094, -1.390032613873701, -0.440875890223325}};
+__constant__ double c_rok4_bs[STX_NSTAGE] = {0.194335256262729, 0.483167813989227, 0.0, 0.322496929748044};
+__constant__ double c_rok4_bt[STX_NSTAGE] = {-0.217819895945721, 1.03130847478467, 0.186511421161047, 0.0};
+
 // The ROK4 integration of one state vector of NV components
 // (rosenbrock_krylov_kernel body, kernels_gpu.F90:10463-10610).  V holds the
 // Krylov basis; the basis handed back (Vb) is its first mA columns.  The
@@ -334,15 +348,10 @@ template <int NV, class F>
 __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, const double *fls, long long fstride,
                           double dttry, double time_start, double time_end, int simpler, int maxsteps) {
   const double gam = 0.572816062482135;
-  const double a21 = 0.432364435748567, a31 = -0.514211316876170, a32 = 1.382271144617360;
-  const double a41 = -0.514211316876170, a42 = 1.382271144617360, a43 = 0.0;
-  const double bs1 = 0.194335256262729, bs2 = 0.483167813989227, bs3 = 0.0, bs4 = 0.322496929748044;
-  const double g21 = -0.602765307997356, g31 = -1.389195789724843, g32 = 1.072950969011413;
-  const double g41 = 0.992356412977094, g42 = -1.390032613873701, g43 = -0.440875890223325;
-  const double bt1 = -0.217819895945721, bt2 = 1.03130847478467, bt3 = 0.186511421161047, bt4 = 0.0;
-  const double alpha[4][3] = {{0, 0, 0}, {a21, 0, 0}, {a31, a32, 0}, {a41, a42, a43}};
-  const double gmc[4][3] = {{0, 0, 0}, {g21, 0, 0}, {g31, g32, 0}, {g41, g42, g43}};
-  const double bsv[4] = {bs1, bs2, bs3, bs4}, btv[4] = {bt1, bt2, bt3, bt4};
+  // the Arnoldi matrices live in the stage vectors 2..4 (dead until the
+  // stages) where they fit, else in arrays of their own
+  constexpr int NH = (STX_MMAX + 1) * STX_MMAX, NI = STX_MMAX * STX_MMAX;
+  constexpr bool HK = 3 * NV >= NH + NI;
   double V[NV * (STX_MMAX + 1)];
   double inv[STX_MMAX * STX_MMAX];
   double Ks[NV * STX_NSTAGE];                // Ks[0..NV) holds f(VEC) until stage 1 replaces it
@@ -362,7 +371,9 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
     // ---- arnoldi (:10664-10792)
     {
       const double TOL = 1e-6, eps = 1.0e-08;
-      double HH[(STX_MMAX + 1) * STX_MMAX], HI[STX_MMAX * STX_MMAX], prj[STX_MMAX], lam[STX_MMAX];
+      double HHo[HK ? 1 : NH], HIo[HK ? 1 : NI];
+      double *HH = HK ? Ks + NV : HHo, *HI = HK ? Ks + NV + NH : HIo;
+      double prj[STX_MMAX], lam[STX_MMAX];
 #pragma unroll
       for (int q = 0; q < (STX_MMAX + 1) * STX_MMAX; q++) HH[q] = 0.0;
 #pragma unroll
@@ -443,13 +454,13 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
         for (int m = 0; m < NV; m++) ys[m] = VEC[m];
 #pragma unroll 1
         for (int jj = 1; jj <= ii - 1; jj++)
-          for (int m = 0; m < NV; m++) ys[m] = ys[m] + dt * alpha[ii - 1][jj - 1] * Ks[(jj - 1) * NV + m];
+          for (int m = 0; m < NV; m++) ys[m] = ys[m] + dt * c_rok4_alpha[ii - 1][jj - 1] * Ks[(jj - 1) * NV + m];
         f.rhs(ys, T_iter, Fv);
       }
       for (int m = 0; m < NV; m++) GK[m] = 0.0;
 #pragma unroll 1
       for (int jj = 1; jj <= ii - 1; jj++)
-        for (int m = 0; m < NV; m++) GK[m] = GK[m] + gmc[ii - 1][jj - 1] / gam * Ks[(jj - 1) * NV + m];
+        for (int m = 0; m < NV; m++) GK[m] = GK[m] + c_rok4_gmc[ii - 1][jj - 1] / gam * Ks[(jj - 1) * NV + m];
       for (int m = 0; m < NV; m++) Fv[m] = Fv[m] + GK[m];
       if (simpler == 1)
         for (int m = 0; m < NV; m++) Fv[m] = Fv[m] - fsav(m);
@@ -483,8 +494,8 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
     for (int ll = 0; ll < NV; ll++) {
       double a = VEC[ll], b = VEC[ll];
       for (int ii = 0; ii < STX_NSTAGE; ii++) {
-        a = a + dt * bsv[ii] * Ks[ii * NV + ll];
-        b = b + dt * btv[ii] * Ks[ii * NV + ll];
+        a = a + dt * c_rok4_bs[ii] * Ks[ii * NV + ll];
+        b = b + dt * c_rok4_bt[ii] * Ks[ii * NV + ll];
       }
       ys[ll] = a;
       const double ev = (b - a) / ((1.0e-4) * a + 1.0e-8);
