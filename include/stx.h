@@ -334,7 +334,8 @@ typedef struct stx_tuning {
   int32_t batch_ctas_max;    /* most CTAs of one stx_batch0d_integrate launch; 0: no cap (a server running
                                 several reactor launches at once caps each, leaving room for other work) */
   float sweep_ms[3];         /* out (stx_autotune): time of the chosen sweep kernels, ms */
-  float chem_ms;             /* out (stx_autotune): time of the chosen chemistry launch, ms */
+  float chem_ms;             /* out (stx_autotune): time of the chosen chemistry launch, ms (stx_autotune tries
+                                the persistent CTA counts from the limit down, then the plain launch) */
 } stx_tuning;
 int stx_get_tuning(stx_ctx *ctx, stx_tuning *out);
 int stx_set_tuning(stx_ctx *ctx, const stx_tuning *t);

@@ -1078,7 +1078,9 @@ int stx_autotune(stx_ctx *c, void *sv, const stx_fields *f, double dt_chem, stx_
     c->weno_list[d] = pick.list;
     sweep_ms[d] = best;
   }
-  // ---- cell chemistry (ROK4): persistent CTAs per SM, on a scratch copy of w
+  // ---- cell chemistry (ROK4), on a scratch copy of w: persistent CTAs per SM
+  // (work stealing), then the plain launch (one thread per cell, -1), which the
+  // hardware's block scheduler balances instead
   const stx_params &p = c->par;
   if (rc == STX_OK && p.enable_chemistry == 2 && p.rosenbrock_version == 2 && dt_chem > 0.0) {
     if (cudaMallocFromPoolAsync((void **)&w2, nw * sizeof(double), pool, s) != cudaSuccess) {
@@ -1087,7 +1089,8 @@ int stx_autotune(stx_ctx *c, void *sv, const stx_fields *f, double dt_chem, stx_
       const int lim = chem_ctas_limit(c->ns);
       float best = -1.f;
       int pick = 0;
-      for (int k = lim; k >= 1 && rc == STX_OK; k--) {     // the default (the limit) first
+      for (int k = lim; k >= -1 && rc == STX_OK; k--) {    // the default (the limit) first
+        if (k == 0) continue;
         c->d.p.chem_ctas_per_sm = k;
         float ms = time_launches(s, e0, e1, 1, [&] {
           if (cudaMemcpyAsync(w2, f->w, nw * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)

@@ -53,7 +53,7 @@ def test_autotune_leaves_fields_and_keeps_a_valid_choice(tmp_path):
     assert s.status(reset=False) == st0
     assert not t["cached"]
     assert all(k in (0, 1) for k in t["sweep_kind"] + t["weno_list"])
-    assert 0 <= t["chem_ctas_per_sm"] <= t["chem_ctas_max"] and t["chem_ctas_max"] >= 1
+    assert -1 <= t["chem_ctas_per_sm"] <= t["chem_ctas_max"] and t["chem_ctas_max"] >= 1
     assert all(ms > 0 for ms in t["sweep_ms"]) and t["chem_ms"] > 0
     got = s.tuning()
     assert got["sweep_kind"] == t["sweep_kind"] and got["weno_list"] == t["weno_list"]
