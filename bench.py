@@ -510,6 +510,7 @@ def cpu_reactors(args, n_sample):
 
 
 def run_reactors(args):
+    import numpy as np
     import torch
     import torch.distributed as dist
     from stx.reactors import BatchReactors, sample_h2air
@@ -522,6 +523,9 @@ def run_reactors(args):
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     br = BatchReactors("h2air_9sp", device=str(dev))
+    split = args.precision == "mixed"
+    if split:
+        br.set_form("split")
     T0, p0, Y0 = sample_h2air(args.reactors, args.seed + rank, br.mech)
     dT0, dp0, dY0 = (torch.as_tensor(a, dtype=torch.float64, device=dev).contiguous() for a in (T0, p0, Y0))
 
@@ -579,6 +583,28 @@ def run_reactors(args):
     # where ROK4's steps stay small -- the oracle caps the same ones)
     capped = nsteps > args.max_steps
     done = int((~capped).sum())
+    err = None
+    if split:
+        # the same reactors once more in the FP64 form: the split form's difference
+        # over the reactors both forms solve
+        o_sp = {k: v.clone() for k, v in out.items()}
+        br.set_form("fp64")
+        o_64 = solve()
+        torch.cuda.synchronize()
+        br.set_form("split")
+        a, b = o_sp["nsteps"].cpu().numpy(), o_64["nsteps"].cpu().numpy()
+        both = (a <= args.max_steps) & (b <= args.max_steps)
+        Ts, T6 = o_sp["T"].cpu().numpy()[both], o_64["T"].cpu().numpy()[both]
+        ts, t6 = o_sp["t_ign"].cpu().numpy()[both], o_64["t_ign"].cpu().numpy()[both]
+        ig = (ts > 0) & (t6 > 0)
+        Ys, Y6 = o_sp["Y"].cpu().numpy()[:, both], o_64["Y"].cpu().numpy()[:, both]
+        big = Y6 > 1e-3
+        err = {"reactors_compared": int(both.sum()),
+               "T_final_rel_max": float(np.max(np.abs(Ts - T6) / T6)) if both.any() else None,
+               "t_ign_rel_median": float(np.median(np.abs(ts[ig] - t6[ig]) / t6[ig])) if ig.any() else None,
+               "t_ign_rel_max": float(np.max(np.abs(ts[ig] - t6[ig]) / t6[ig])) if ig.any() else None,
+               "Y_gt_1e-3_rel_max": float(np.max(np.abs(Ys[big] - Y6[big]) / Y6[big])) if big.any() else None,
+               "steps_ratio_mean": float(np.mean(a[both] / np.maximum(b[both], 1)))}
     line = {"metric": R_METRIC, "value": done * world * args.steps / (ms_max / 1e3), "unit": R_METRIC,
             "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -595,6 +621,11 @@ def run_reactors(args):
                     "path": "BatchReactors.integrate -> stx_batch0d_integrate, inputs from and outputs to pinned "
                             "host memory every step"},
             "status_bits": status}
+    line["config"]["precision_form"] = ("FP32/FP64 split (ROK4 Krylov basis and stage vectors in FP32; state, "
+                                        "right-hand sides and error control in FP64)") if split else "plain FP64"
+    if split:
+        line["dtype"] = "f32/f64 split"
+        line["error_vs_fp64"] = err
     if world == 1 and rank == 0 and not args.no_cpu:
         rate, cores, sample = cpu_reactors(args, 64)
         line["cpu_baseline"] = {"value": rate, "unit": R_METRIC, "cores": cores, "kind": "port", "sample": sample}

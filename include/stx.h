@@ -284,7 +284,11 @@ int stx_graph_destroy(stx_graph *g);
  * t_ign (first accepted time with T > ign_factor T0, or -1), t_end (time
  * reached), nsteps (ROK4 steps).  Integration ends at min(t_max,
  * end_factor t_ign); max_steps caps the steps of each reactor
- * (STX_ST_ROS_STEPS_CAP).  Uses the context's tables and work counter. */
+ * (STX_ST_ROS_STEPS_CAP).  Uses the context's tables and work counter.  With
+ * the context in the mixed precision form (stx_set_precision) the reactors run
+ * the FP32/FP64-split form: the Krylov basis and the stage vectors stored in
+ * FP32, the state, every right-hand side and the error control in FP64 (one
+ * thread per reactor for every batch size). */
 int stx_batch0d_integrate(stx_ctx *ctx, void *stream, int n, const double *T0, const double *p0, const double *Y0,
                           double t_max, double dttry, double ign_factor, double end_factor, int max_steps, double *Y,
                           double *T, double *t_ign, double *t_end, int32_t *nsteps);

@@ -734,9 +734,12 @@ int stx_batch0d_integrate(stx_ctx *c, void *s, int n, const double *T0, const do
   // reactor gets a resident warp at once: a warp integrates one reactor several
   // times faster than a thread, so a small batch (a served one) ends sooner.
   // Larger batches run a thread per reactor (more reactors at once).
-  // STX_BATCH0D_KERNEL=thread / warp forces either kernel.
+  // STX_BATCH0D_KERNEL=thread / warp forces either kernel.  In the mixed
+  // precision form (stx_set_precision) the reactors run the thread kernel's
+  // FP32/FP64-split form: the Krylov basis and stage vectors in FP32, the state,
+  // every right-hand side and the error control in FP64.
   const char *kind = std::getenv("STX_BATCH0D_KERNEL");
-  if (!(kind && std::strcmp(kind, "thread") == 0)) {
+  if (!(kind && std::strcmp(kind, "thread") == 0) && !c->d.p.mixed) {
     int force = kind && std::strcmp(kind, "warp") == 0;
     int rc = launch_batch0d_warp(d, S(s), n, T0, p0, Y0, t_max, dttry, ign_factor, end_factor, Y, T, t_ign, t_end,
                                  nsteps, c->counter_d, force);

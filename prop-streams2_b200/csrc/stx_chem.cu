@@ -63,7 +63,9 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
 // times, so their step counts differ by orders of magnitude).  Y0 / Y are
 // (n, ns) with the reactor index fastest.  cg: the device-resident context (the
 // right-hand side takes it by reference, see k_rok4); maxsteps: the step cap.
-template <int NS>
+// A: the storage of the Krylov basis and stage vectors (double; float for the
+// FP32/FP64-split form, rok4_core).
+template <int NS, typename A = double>
 __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
     k_batch0d(const DevCtx *__restrict__ cg, int maxsteps, int n, const double *__restrict__ T0,
               const double *__restrict__ p0,
@@ -82,7 +84,7 @@ __global__ void __launch_bounds__(chem_block(NS), STX_ROK4_MINB)
 #pragma unroll 1
     for (int k = 0; k < NS; k++) h = h + VEC[k] * species_poly_int(c.t, c.t.cpi, T0r, k + 1);
     Rok4ConstP<NS> f{c, h, p0[r], T0r, ign_factor, end_factor, -1.0, 0.0, T0r, 0};
-    rok4_core<NS>(c, f, VEC, T0r, nullptr, 0, dttry, 0.0, t_max, 0, maxsteps);
+    rok4_core<NS, Rok4ConstP<NS>, A>(c, f, VEC, T0r, nullptr, 0, dttry, 0.0, t_max, 0, maxsteps);
 #pragma unroll
     for (int k = 0; k < NS; k++) Y[(long long)k * n + r] = VEC[k];
     T[r] = f.T_final;
@@ -411,12 +413,19 @@ static int batch0d_t(const DevCtx &c, const DevCtx *cg, cudaStream_t s, int n, c
                      double t_max, double dttry, double ign, double endf, double *Y, double *T, double *t_ign,
                      double *t_end, int *nsteps, unsigned int *counter) {
   STX_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
-  int nb = persistent_blocks((const void *)k_batch0d<NS>, chem_block(NS));
+  // the context's mixed precision form selects the FP32/FP64-split reactors
+  const bool split = c.p.mixed != 0;
+  int nb = persistent_blocks(split ? (const void *)k_batch0d<NS, float> : (const void *)k_batch0d<NS>,
+                             chem_block(NS));
   long long need = ((long long)n + chem_block(NS) - 1) / chem_block(NS);
   if (nb > need) nb = (int)need;
   if (c.p.batch_ctas_max > 0 && nb > c.p.batch_ctas_max) nb = c.p.batch_ctas_max;
-  k_batch0d<NS><<<nb, chem_block(NS), 0, s>>>(cg, c.p.ros_maxsteps, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T,
-                                              t_ign, t_end, nsteps, counter);
+  if (split)
+    k_batch0d<NS, float><<<nb, chem_block(NS), 0, s>>>(cg, c.p.ros_maxsteps, n, T0, p0, Y0, t_max, dttry, ign, endf,
+                                                       Y, T, t_ign, t_end, nsteps, counter);
+  else
+    k_batch0d<NS><<<nb, chem_block(NS), 0, s>>>(cg, c.p.ros_maxsteps, n, T0, p0, Y0, t_max, dttry, ign, endf, Y, T,
+                                                t_ign, t_end, nsteps, counter);
   STX_CUDA_TRY(cudaGetLastError());
   return STX_OK;
 }

@@ -2,6 +2,7 @@
 // by the kernels of stx_chem.cu: production rates, the ROK4 Krylov cell update
 // (kernels_gpu.F90:10360-11205) and the work-stealing cell claim.
 #pragma once
+#include <type_traits>
 #include "stx_kernels.cuh"
 
 // Linkage of the ROK4 right-hand side: one out-of-line copy (default).  Inlined
@@ -344,19 +345,29 @@ __constant__ double c_rok4_bt[STX_NSTAGE] = {-0.217819895945721, 1.0313084747846
 // temperature guess is the same, reuses it with the operations the reference
 // applies to a fresh evaluation (f(VEC) + 0 - fl_sav), so the result is the
 // same bit for bit with one right-hand side fewer per step.
-template <int NV, class F>
+//
+// A: the storage of the Krylov basis V and the stage vectors Ks -- double (the
+// reference method), or float for the FP32/FP64-split form of the batched
+// reactors, where the state, every right-hand side (T from h, rates, K_c), the
+// finite-difference Jacobian products, the small Krylov matrices and the error
+// norm stay FP64 and only those two arrays are rounded to FP32.  f(VEC), which
+// the finite differences subtract, is then kept in the FP64 scratch S2.
+template <int NV, class F, typename A = double>
 __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, const double *fls, long long fstride,
                           double dttry, double time_start, double time_end, int simpler, int maxsteps) {
   const double gam = 0.572816062482135;
+  constexpr bool AD = std::is_same<A, double>::value;
   // the Arnoldi matrices live in the stage vectors 2..4 (dead until the
   // stages) where they fit, else in arrays of their own
   constexpr int NH = (STX_MMAX + 1) * STX_MMAX, NI = STX_MMAX * STX_MMAX;
-  constexpr bool HK = 3 * NV >= NH + NI;
-  double V[NV * (STX_MMAX + 1)];
+  constexpr bool HK = AD && 3 * NV >= NH + NI;
+  A V[NV * (STX_MMAX + 1)];
   double inv[STX_MMAX * STX_MMAX];
-  double Ks[NV * STX_NSTAGE];                // Ks[0..NV) holds f(VEC) until stage 1 replaces it
+  A Ks[NV * STX_NSTAGE];                     // Ks[0..NV) holds f(VEC) until stage 1 replaces it (A = double)
   double S0[NV], S1[NV], S2[NV];             // scratch: jac / wl, then ys / F / GK, then the new state
-  double *raw = Ks;
+  double *raw;
+  if constexpr (AD) raw = Ks;
+  else raw = S2;
   auto fsav = [&](int m) -> double { return fls[(long long)m * fstride]; };
   // rhs_sav of the reference: f(VEC), less fl_sav with the simpler splitting
   auto rhs_sav = [&](int m) -> double { return simpler == 1 ? raw[m] - fsav(m) : raw[m]; };
@@ -372,7 +383,14 @@ __device__ void rok4_core(const DevCtx &c, F &f, double *VEC, double T_iter, con
     {
       const double TOL = 1e-6, eps = 1.0e-08;
       double HHo[HK ? 1 : NH], HIo[HK ? 1 : NI];
-      double *HH = HK ? Ks + NV : HHo, *HI = HK ? Ks + NV + NH : HIo;
+      double *HH, *HI;
+      if constexpr (HK) {
+        HH = Ks + NV;
+        HI = Ks + NV + NH;
+      } else {
+        HH = HHo;
+        HI = HIo;
+      }
       double prj[STX_MMAX], lam[STX_MMAX];
 #pragma unroll
       for (int q = 0; q < (STX_MMAX + 1) * STX_MMAX; q++) HH[q] = 0.0;

@@ -128,6 +128,14 @@ class BatchReactors:
                                              vp(out["t_ign"]), vp(out["t_end"]), vp(out["nsteps"])),
               "stx_batch0d_integrate")
 
+    def set_form(self, form: str):
+        """"fp64" (the reference method, default) or "split": the FP32/FP64-split
+        form, with the Krylov basis and the stage vectors of ROK4 stored in FP32
+        and the state, every right-hand side and the error control in FP64 (the
+        context's mixed precision form)."""
+        mode = {"fp64": 0, "split": 1}[form]
+        check(self.lib.stx_set_precision(self.ctx, mode), "stx_set_precision")
+
     def set_launch_cap(self, ctas: int):
         """Cap the CTAs of this context's launches (0: none), so that several
         reactor launches running at once leave SMs for other work: the
