@@ -317,8 +317,8 @@ int stx_batch0d_integrate(stx_ctx *ctx, void *stream, int n, const double *T0, c
  * So that no call allocates, a call whose kernel needs more than the current
  * limit launches nothing and returns STX_E_LOCAL_MEM.  Raise the limit once at
  * initialisation, e.g. cudaDeviceSetLimit(cudaLimitStackSize, 4608) for up to
- * 14 species or 12288 for 53 (this build's frames: 2704 B at 9 species, 3488 B
- * at 14, 10432 B at 53; the call checks the kernel's actual figure). */
+ * 14 species or 12288 for 53 (this build's frames: 2624 B at 9 species, 3360 B
+ * at 14, 9744 B at 53; the call checks the kernel's actual figure). */
 int stx_rosenbrock_krylov_noalloc(const stx_params *par, const stx_tables *tab_dev, const stx_grid *grid,
                                   void *stream, double *w, const double *w_aux, const double *fl_sav,
                                   double dttry, double time_start, double time_end, int simpler, uint32_t *status);

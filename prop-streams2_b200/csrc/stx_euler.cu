@@ -665,13 +665,23 @@ __global__ void __launch_bounds__(YZ_TI * YZ_TF) k_euler_yz(DevCtx c, const DevC
 // 39 KB of shared memory also admits 5) ran an x sweep of a developed 128^3
 // field in 0.585 ms against 0.679 ms at 4 (128 registers), with the same
 // results bit for bit.  y and z: 2, where their 91 KB of shared memory also
-// sets the limit
+// sets the limit.  y / z tiles of 8 lines at 4 CTAs per SM (128 registers)
+// ran the y and z sweeps of a developed 256^3 field in 2.84 ms against 2.73 ms
+// at 16 lines, and in 3.23 ms at 3 CTAs per SM (168 registers), the same bits
 #ifndef STX_ETILE_X_MINB
 #define STX_ETILE_X_MINB 5
 #endif
+// lines (consecutive i) per CTA of the y / z tiles, and the CTAs per SM their
+// register budget is sized for
+#ifndef STX_ETILE_YZ_NL
+#define STX_ETILE_YZ_NL 16
+#endif
+#ifndef STX_ETILE_YZ_MINB
+#define STX_ETILE_YZ_MINB 2
+#endif
 template <int NS, int DIR, bool TMA = false> struct ETile {
   static constexpr int TC = DIR == 0 ? 64 : 16;        // cells per line updated by a CTA
-  static constexpr int NL = DIR == 0 ? 2 : 16;         // lines per CTA
+  static constexpr int NL = DIR == 0 ? 2 : STX_ETILE_YZ_NL;   // lines per CTA
   static constexpr int H = 3;                          // halo cells each side
   static constexpr int S = TC + 2 * H;                 // staged cells per line
   static constexpr int NF = TC + 1;                    // faces per line
@@ -777,7 +787,7 @@ __device__ __forceinline__ int etile_field(int v) {
 // out-of-bounds fill), as the loads of the plain staging give them.
 // Everything after the staging is the same code on the same values.
 template <int NS, int DIR, typename R, bool TMA = false>
-__global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MINB : 2)
+__global__ void __launch_bounds__(ETile<NS, DIR>::NT, DIR == 0 ? STX_ETILE_X_MINB : STX_ETILE_YZ_MINB)
     k_euler_tile(DevCtx c, const DevCtx *__restrict__ cg, const double *__restrict__ wa, double *__restrict__ fl,
                  int nmin, int nmax, int overwrite, const double *__restrict__ fhw, long long cap,
                  const __grid_constant__ CUtensorMap tmap) {
