@@ -89,7 +89,7 @@ def turbulence_velocity(n: int, seed: int, k0: float = 4.0, xp=np, device=None):
         dot = (kx * comps[0] + ky * comps[1] + kz * comps[2]) / kd
         out = []
         for a, kc in zip(comps, (kx, ky, kz)):
-            out.append(np.fft.irfftn(a - kc * dot, s=(n, n, n)))
+            out.append(np.fft.irfftn(a - kc * dot, s=(n, n, n), axes=(0, 1, 2)))
         return out
     import torch
     g = torch.Generator(device=device).manual_seed(seed)
