@@ -84,3 +84,62 @@ def test_turbulence_state_has_the_stated_mean_state_and_rms():
     # a same-resolution sample: the grid spacing is that of the 256^3 box
     for xg in case.xg:
         np.testing.assert_allclose(np.diff(xg), 2.0 * math.pi * p["ell"] / 256, rtol=1e-12)
+
+
+def test_stiff_mechanism_has_the_stated_distributions():
+    """The 53-species / 325-reaction workload: A ~ logU(1e8, 1e16) (cm, mol
+    units), b ~ U(-1.5, 2), Ea ~ U(0, 50) kcal/mol, about 20 % three-body
+    reactions with efficiencies U(0.5, 5); every reaction reversible and
+    bimolecular between four distinct species of one molecular weight; NASA-7
+    coefficients within 5 % of N2's."""
+    mech = M.synthetic_mechanism(53, 325, 0)
+    assert len(mech.species) == 53 and len(mech.reactions) == 325
+    mw = {s.mw for s in mech.species}
+    assert len(mw) == 1
+    n2 = [[3.298677, 0.0014082404, -3.963222e-06, 5.641515e-09, -2.444854e-12, -1020.8999, 3.950372],
+          [2.92664, 0.0014879768, -5.68476e-07, 1.0097038e-10, -6.753351e-15, -922.7977, 5.980528]]
+    for s in mech.species:
+        r = np.array(s.coeffs) / np.array(n2)
+        assert r.min() >= 0.95 and r.max() <= 1.05
+    cal = 4.184e6
+    three = 0
+    for r in mech.reactions:
+        assert r.reversible
+        names = list(r.reactants) + list(r.products)
+        assert len(set(names)) == 4 and all(v == 1.0 for v in list(r.reactants.values()) + list(r.products.values()))
+        A, b, Ea = r.rate
+        if r.efficiencies is not None:
+            three += 1
+            A_cgs = A / (1e-6 / 1e-3) ** 2
+            effs = np.array(list(r.efficiencies.values()))
+            assert len(effs) == 53 and effs.min() >= 0.5 and effs.max() <= 5.0
+        else:
+            A_cgs = A / (1e-6 / 1e-3)
+        assert 8.0 <= math.log10(A_cgs) <= 16.0
+        assert -1.5 <= b <= 2.0 and 0.0 <= Ea / cal <= 50.0
+    assert 0.14 < three / 325 < 0.26
+    assert M.synthetic_mechanism(53, 325, 0).reactions[17].rate == mech.reactions[17].rate
+
+
+def test_stiff_case_state():
+    """The 53-species box: p = 1 atm at rest, T a smooth seeded field spanning
+    1200..2000 K, Y_k ~ Dirichlet(0.5) per cell."""
+    n = 8
+    mech, tables = configs.stiff_mechanism_tables(0)
+    case = configs.stiff_case(n, tables=tables)
+    ns, ng = case.ns, case.ng
+    assert ns == 53 and case.nv == 57
+    sl = (slice(ng, ng + n),) * 3
+    w = case.w
+    rho = w[(slice(0, ns),) + sl].sum(axis=0)
+    Y = w[(slice(0, ns),) + sl] / rho[None]
+    assert Y.min() >= 0.0 and np.max(np.abs(Y.sum(axis=0) - 1.0)) < 1e-13
+    # Dirichlet(0.5) over 53 species: E[Y_k] = 1/53, Var = (1/53)(52/53)/(53*0.5 + 1)
+    assert abs(Y.mean() - 1.0 / 53) < 1e-12
+    assert abs(Y.var() / ((1.0 / 53) * (52.0 / 53) / 27.5) - 1.0) < 0.1
+    for m in range(3):
+        assert np.all(w[(ns + m,) + sl] == 0.0)
+    T = case.w_aux[(case.J("T"),) + sl]
+    assert T.min() >= 1200.0 - 1e-9 and T.max() <= 2000.0 + 1e-9 and T.max() - T.min() > 600.0
+    rm = np.einsum("k,kzyx->zyx", tables.rgas, Y)
+    np.testing.assert_allclose(rho * rm * T, 101325.0, rtol=1e-12)
