@@ -1,8 +1,10 @@
-"""The synthetic turbulence workload, built on the host (numpy and torch on the
-CPU), against its description: a random-phase solenoidal velocity with
-E(k) ~ k^4 exp(-2 (k/k0)^2), k0 = 4, scaled to u_rms = 0.3 c0 of the mean
-state (9-species H2/air, phi = 0.7, T = 1000 K, p = 1 atm), on a box whose
-ghost points hold the mean state at rest."""
+"""The workloads' inputs, built on the host, against their descriptions:
+  * the turbulence box (numpy and torch on the CPU): a random-phase solenoidal
+    velocity with E(k) ~ k^4 exp(-2 (k/k0)^2), k0 = 4, scaled to u_rms = 0.3 c0
+    of the mean state (9-species H2/air, phi = 0.7, T = 1000 K, p = 1 atm), the
+    ghost points holding the mean state at rest;
+  * the 53-species / 325-reaction stiff mechanism and its box;
+  * the 2400-cell reactive shock tube's initial state."""
 import math
 
 import numpy as np
@@ -143,3 +145,51 @@ def test_stiff_case_state():
     assert T.min() >= 1200.0 - 1e-9 and T.max() <= 2000.0 + 1e-9 and T.max() - T.min() > 600.0
     rm = np.einsum("k,kzyx->zyx", tables.rgas, Y)
     np.testing.assert_allclose(rho * rm * T, 101325.0, rtol=1e-12)
+
+
+def _T_from_e(tb, e, Y, lo=200.0, hi=5000.0):
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if M.mixture_e(tb, mid, Y) < e:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def test_config1_shock_tube_initial_state():
+    """The 2400-cell reactive shock tube: H2:O2:Ar = 2:1:7 by moles over 0.12 m,
+    left state rho = 0.072 kg/m^3, p = 7173 Pa at rest, right state (x >= 0.06 m)
+    rho = 0.18075 kg/m^3, p = 35594 Pa, u = -487.34 m/s."""
+    c = configs.config1_case(2400)
+    ns, ng, nx = c.ns, c.ng, c.nx
+    assert nx == 2400 and c.cfl == 0.5
+    x = np.asarray(c.x)[ng:ng + nx]
+    assert x[0] == 0.0 and abs(x[-1] - 0.12) < 1e-15
+    w = c.w[:, ng, ng, ng:ng + nx]
+    rho = w[:ns].sum(axis=0)
+    Y = w[:ns] / rho[None]
+    mech = configs.mechanism("shock_tube_9sp")
+    mw = np.array([s.mw for s in mech.species])
+    X = Y / mw[:, None]
+    X = X / X.sum(axis=0)
+    # the example's mass fractions (multideal.ini init_Y_*), which are 2:1:7 by
+    # moles to within 0.7 %
+    for k in range(ns):
+        np.testing.assert_allclose(Y[k], float(configs.TUBE_INI["ref_state"]["init_Y_%02d" % (k + 1)]),
+                                   rtol=1e-13, atol=1e-16)
+    for name, frac in (("H2", 0.2), ("O2", 0.1), ("AR", 0.7)):
+        k = [s.name.upper() for s in mech.species].index(name)
+        np.testing.assert_allclose(X[k], frac, rtol=7e-3)
+    right = x >= 0.06
+    assert right.sum() == nx // 2
+    u = w[ns] / rho
+    tb = c.tb
+    for sel, r0, u0, p0 in ((~right, 0.072, 0.0, 7173.0), (right, 0.18075, -487.34, 35594.0)):
+        i = np.flatnonzero(sel)[[0, -1]]
+        np.testing.assert_allclose(rho[i], r0, rtol=1e-14)
+        np.testing.assert_allclose(u[i], u0, rtol=1e-14, atol=1e-14)
+        for j in i:
+            e = w[ns + 3, j] / rho[j] - 0.5 * u[j] ** 2
+            T = _T_from_e(tb, e, Y[:, j])
+            assert abs(rho[j] * float(np.dot(tb.rgas, Y[:, j])) * T / p0 - 1.0) < 1e-9
