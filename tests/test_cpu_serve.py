@@ -8,7 +8,7 @@ import numpy as np
 import helpers as H  # noqa: F401  (puts the package on sys.path)
 from stx import configs
 from stx.reactors import sample_h2air
-from stx.serve import mixed_requests
+from stx.requests import mixed_requests
 
 MECH = configs.mechanism("h2air_9sp")
 
